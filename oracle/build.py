@@ -1,0 +1,78 @@
+"""Oracle build recipes — TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__`` and ``bench.py``'s CPU-baseline legs use the
+oracle; the product never imports it.
+
+* ``build_oracle()`` compiles the C restatement ``walk_oracle.c`` into
+  ``oracle/liboracle.so`` (gcc, OpenMP, ``-ffp-contract=off`` so that the
+  single-precision walk rounds every operation as the reference source reads).
+* ``build_reference_kernel(code)`` compiles the reference's own kernel source
+  (``simulation_toolkit/simulation_engine/sim3d_kernel.cu``), after the same
+  ``%``-template substitution the reference performs at diffsim3d.py:39, as C++
+  for the CPU with the host stand-ins in ``oracle/refshim`` and the launch
+  emulation ``refshim/harness.cpp``.  Outputs go to ``oracle/_ref/`` only; the
+  reference source is read where it lies and never copied into the repository.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import subprocess
+from pathlib import Path
+
+ORACLE_DIR = Path(__file__).resolve().parent
+REF_OUT = ORACLE_DIR / "_ref"
+ORACLE_SO = ORACLE_DIR / "liboracle.so"
+REFERENCE_ROOT = Path(os.environ.get("NOZOMI_REFERENCE_ROOT", "/root/reference"))
+REF_KERNEL_REL = "simulation_toolkit/simulation_engine/sim3d_kernel.cu"
+
+_ORACLE_SRC = [ORACLE_DIR / "walk_oracle.c", ORACLE_DIR / "walk_step.inc", ORACLE_DIR / "oz_rng.h"]
+
+
+def _stale(target: Path, sources) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(s.stat().st_mtime > t for s in sources)
+
+
+def build_oracle(force: bool = False) -> Path:
+    """Compile oracle/liboracle.so if missing or older than its sources."""
+    if force or _stale(ORACLE_SO, _ORACLE_SRC):
+        cmd = ["gcc", "-O3", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+               "-Wall", "-o", str(ORACLE_SO), str(ORACLE_DIR / "walk_oracle.c"), "-lm"]
+        subprocess.run(cmd, check=True)
+    return ORACLE_SO
+
+
+def reference_available() -> bool:
+    return (REFERENCE_ROOT / REF_KERNEL_REL).is_file()
+
+
+def substitute_reference(pars: dict) -> str:
+    """The reference's kernel source with its template constants filled in,
+    exactly as ``self.code % self.pars`` does (diffsim3d.py:39)."""
+    return (REFERENCE_ROOT / REF_KERNEL_REL).read_text() % pars
+
+
+def build_reference_kernel(code: str) -> Path:
+    """Compile an already-substituted reference kernel source for the CPU."""
+    REF_OUT.mkdir(parents=True, exist_ok=True)
+    shim = ORACLE_DIR / "refshim"
+    tag = hashlib.sha1((code + (shim / "harness.cpp").read_text() + (shim / "curand_kernel.h").read_text()
+                        + (ORACLE_DIR / "oz_rng.h").read_text()).encode()).hexdigest()[:16]
+    so = REF_OUT / f"ref_{tag}.so"
+    if so.exists():
+        return so
+    src = REF_OUT / f"ref_{tag}.cpp"
+    src.write_text(code)
+    cmd = ["g++", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-w",
+           "-I", str(shim), "-x", "c++", str(src), "-x", "c++", str(shim / "harness.cpp"),
+           "-o", str(so) + ".tmp"]
+    subprocess.run(cmd, check=True)
+    os.replace(str(so) + ".tmp", so)
+    return so
+
+
+if __name__ == "__main__":
+    print(build_oracle(force=True))

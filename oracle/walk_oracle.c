@@ -1,0 +1,341 @@
+/*
+ * Oracle — TEST INFRASTRUCTURE ONLY.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs load
+ * this library, and only as the checker or as the timed CPU baseline; the
+ * product (nozomi_b200) never links, loads or calls it.
+ *
+ * CPU restatement of nozomi's Monte Carlo spin random walk
+ * (simulation_toolkit/simulation_engine/sim3d_kernel.cu):
+ *   sphere tests / ray-sphere fractions   sim3d_kernel.cu:72-160
+ *   rejection seeding rule                sim3d_kernel.cu:240-337, geometry.py:73-174
+ *   walk with T2 weighting                sim3d_kernel.cu:340-522
+ *   walk with multi-direction phase       sim3d_kernel.cu:719-943
+ *   displacement moments                  sim3d_kernel.cu:162-238
+ * The single-precision walk evaluates the reference's expressions in source
+ * order with IEEE rounding and no contraction (built with -ffp-contract=off),
+ * so with the same draws it reproduces the reference bit for bit; the pin is
+ * tests/test_oracle_pin.py against fixtures that the reference's own Python
+ * driver and kernel source produced (tests/golden/make_golden.py).
+ *
+ * Walkers are independent, so the oracle runs walker by walker (all steps of
+ * one walker, then the next), split over OpenMP threads.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include "oz_rng.h"
+
+#define OZ_API __attribute__((visibility("default")))
+
+#define OZ_TOL ((float)1e-4) /* sim3d_kernel.cu:34 const float tol = 1e-4 */
+#define OZ_BIG ((float)1e6)  /* sim3d_kernel.cu:35 someLargeNumber */
+
+#define OZ_MIN(a, b) (((a) > (b)) ? (b) : (a)) /* sim3d_kernel.cu:7 */
+#define OZ_MAX(a, b) (((a) < (b)) ? (b) : (a)) /* sim3d_kernel.cu:8 */
+
+enum {
+    OZ_MODE_SIG = 1,        /* T2 weighting of sig (randomWalk3d) */
+    OZ_MODE_PHASE = 2,      /* per-direction phase (randomWalk3d_phase_multidirr) */
+    OZ_MODE_PHI = 4,        /* Kahan 3-vector Phi = sum G_n p_n */
+    OZ_MODE_TANGENT64 = 8,  /* FP64 near-tangent solves */
+};
+enum {
+    OZ_FLAG_DRAWS_EXHAUSTED = 1, /* injected normal table ran out; the draw reads 0 */
+    OZ_FLAG_ITER_CAP = 2,        /* a step ended at the 100-iteration cap */
+    OZ_FLAG_UNSEEDED = 4,        /* seeding gave up after its round limit */
+};
+enum { OZ_RNG_INJECT = 0, OZ_RNG_PHILOX = 1 };
+
+typedef struct oz_geom {
+    int S;              /* spheres */
+    int nstructures;    /* sphere structures; the box is structure nstructures */
+    float Lx, Ly, Lz;   /* box, centred on the origin */
+    float dLx, dLy, dLz;/* cell edge per axis */
+    float nLx, nLy, nLz;/* cells per axis (float, like the reference's constants) */
+    const float* spheres;   /* [5, S] SoA: cx, cy, cz, r, structure id */
+    const int* cell_start;  /* [ncell] */
+    const int* cell_count;  /* [ncell] */
+    const int* cell_items;  /* sphere indices */
+    const float* D;         /* [nstructures + 1] um^2/ms */
+    const float* T2;        /* [nstructures + 1] ms */
+} oz_geom;
+
+typedef struct oz_rng {
+    int kind;               /* OZ_RNG_INJECT or OZ_RNG_PHILOX */
+    const float* normals;   /* injected: [N][nsteps][maxk], k-th normal of a walker's step */
+    int nsteps, maxk;
+    uint32_t key0, key1, stream;
+} oz_rng;
+
+static inline void oz_draw3(const oz_rng* rng, int w, int step, int draw,
+                            float* n0, float* n1, float* n2, int* flags) {
+    if (rng->kind == OZ_RNG_PHILOX) {
+        oz_philox_normal3(rng->key0, rng->key1, rng->stream, (uint32_t)w, (uint32_t)step,
+                          (uint32_t)draw, n0, n1, n2);
+        return;
+    }
+    float v[3];
+    for (int i = 0; i < 3; ++i) {
+        int k = 3 * draw + i;
+        if (step < 0 || step >= rng->nsteps || k >= rng->maxk) {
+            v[i] = 0.0f;
+            if (flags) flags[w] |= OZ_FLAG_DRAWS_EXHAUSTED;
+        } else {
+            v[i] = rng->normals[((size_t)w * rng->nsteps + step) * rng->maxk + k];
+        }
+    }
+    *n0 = v[0]; *n1 = v[1]; *n2 = v[2];
+}
+
+/* Full-FP64 ray-sphere fractions, used by the near-tangent precision form. */
+static double oz_in_tol_f64(double dx, double dy, double dz, double r, double jx, double jy, double jz,
+                            double tol) {
+    if ((dx*dx + dy*dy + dz*dz - r*r) > 0) return 1e6;
+    double a = jx*jx + jy*jy + jz*jz;
+    double b = 2*(jx*dx + jy*dy + jz*dz);
+    double c = dx*dx + dy*dy + dz*dz - (r-tol)*(r-tol);
+    double sqterm = b*b - 4*a*c;
+    if (sqterm < 0) return 0;
+    sqterm = sqrt(sqterm);
+    double q = -0.5*(b + sqterm);
+    if (b < 0) q = -0.5*(b - sqterm);
+    double fpos = q/a, fneg = c/q;
+    return OZ_MAX(OZ_MAX(fpos, fneg), 0);
+}
+
+static double oz_out_tol_f64(double dx, double dy, double dz, double r, double jx, double jy, double jz,
+                             double tol) {
+    double a = jx*jx + jy*jy + jz*jz;
+    double b = 2*(jx*dx + jy*dy + jz*dz);
+    double c = dx*dx + dy*dy + dz*dz - (r+tol)*(r+tol);
+    double sqterm = b*b - 4*a*c;
+    if (sqterm < 0) return 1e6;
+    sqterm = sqrt(sqterm);
+    double q = -0.5*(b + sqterm);
+    if (b < 0) q = -0.5*(b - sqterm);
+    double fpos = q/a, fneg = c/q;
+    if ((dx*dx + dy*dy + dz*dz - r*r) < 0) return OZ_MAX(fpos, fneg);
+    if (fpos > 0 && fneg > 0) return OZ_MIN(fpos, fneg);
+    else if ((fpos < 0 && fneg < 0) || (b > 0)) return 1e6;
+    return 0;
+}
+
+/* ---- single precision, the reference's arithmetic ---- */
+#define REAL float
+#define SFX(name) oz_##name##_f32
+#define RSQRT sqrtf
+#define RFLOOR floorf
+#define REXP expf
+#include "walk_step.inc"
+#undef REAL
+#undef SFX
+#undef RSQRT
+#undef RFLOOR
+#undef REXP
+
+/* ---- full double precision ---- */
+#define REAL double
+#define SFX(name) oz_##name##_f64
+#define RSQRT sqrt
+#define RFLOOR floor
+#define REXP exp
+#include "walk_step.inc"
+#undef REAL
+#undef SFX
+#undef RSQRT
+#undef RFLOOR
+#undef REXP
+
+static int oz_threads(int nthreads) {
+#ifdef _OPENMP
+    return nthreads > 0 ? nthreads : omp_get_max_threads();
+#else
+    (void)nthreads;
+    return 1;
+#endif
+}
+
+/*
+ * Steps [step0, step0 + nsteps) for all N walkers.  G and Garea are indexed by
+ * absolute step (the per-sample arguments of diffsim3d.py:252-255).  Any of
+ * phase, sig, phi, label, n_iter, n_scatter, flags, work may be NULL when the
+ * mode does not need them.  work (length 4, summed over walkers): iterations,
+ * spheres within reach, solves within reach, unused.
+ */
+OZ_API int oz_walk_f32(const oz_geom* g, const oz_rng* rng, int mode, int N, int step0, int nsteps,
+                       float dt, const float* G, const float* Garea,
+                       float* spins, float* spins0, float* phase, const float* diffdir, int ndir,
+                       float* sig, float* phi, int* label, int* n_iter, int* n_scatter, int* flags,
+                       long long* work, int nthreads) {
+    if (!g || !rng || N < 0 || nsteps < 0) return 1;
+    const int nt = oz_threads(nthreads);
+    long long acc0 = 0, acc1 = 0, acc2 = 0;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 64) reduction(+:acc0,acc1,acc2)
+    for (int w = 0; w < N; ++w) {
+        long long wk[4] = {0, 0, 0, 0};
+        for (int s = step0; s < step0 + nsteps; ++s)
+            oz_walker_step_f32(g, rng, mode, N, w, s, dt, G ? G[s] : 0.0f, Garea ? Garea[s] : 0.0f,
+                               spins, spins0, phase, diffdir, ndir, sig, phi, label, n_iter, n_scatter,
+                               flags, work ? wk : NULL);
+        acc0 += wk[0]; acc1 += wk[1]; acc2 += wk[2];
+    }
+    if (work) { work[0] += acc0; work[1] += acc1; work[2] += acc2; }
+    return 0;
+}
+
+OZ_API int oz_walk_f64(const oz_geom* g, const oz_rng* rng, int mode, int N, int step0, int nsteps,
+                       double dt, const double* G, const double* Garea,
+                       double* spins, double* spins0, double* phase, const double* diffdir, int ndir,
+                       double* sig, double* phi, int* label, int* n_iter, int* n_scatter, int* flags,
+                       int nthreads) {
+    if (!g || !rng || N < 0 || nsteps < 0) return 1;
+    const int nt = oz_threads(nthreads);
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 64)
+    for (int w = 0; w < N; ++w)
+        for (int s = step0; s < step0 + nsteps; ++s)
+            oz_walker_step_f64(g, rng, mode, N, w, s, dt, G ? G[s] : 0.0, Garea ? Garea[s] : 0.0,
+                               spins, spins0, phase, diffdir, ndir, sig, phi, label, n_iter, n_scatter,
+                               flags, NULL);
+    return 0;
+}
+
+/*
+ * Label of a point: the lowest structure id among the spheres of its cell list
+ * that contain it, else nstructures (the box).  Shared by seeding.
+ */
+static int oz_label_of(const oz_geom* g, float px, float py, float pz) {
+    const int S = g->S;
+    const float *cx = g->spheres, *cy = cx + S, *cz = cx + 2*S, *rr = cx + 3*S, *sid = cx + 4*S;
+    int idx = (int)(OZ_MIN(g->nLz-1, OZ_MAX(0, floorf((pz+g->Lz/2)/g->dLz)))*g->nLx*g->nLy +
+                    OZ_MIN(g->nLy-1, OZ_MAX(0, floorf((py+g->Ly/2)/g->dLy)))*g->nLx +
+                    OZ_MIN(g->nLx-1, OZ_MAX(0, floorf((px+g->Lx/2)/g->dLx))));
+    int label = g->nstructures;
+    const int* items = g->cell_items + g->cell_start[idx];
+    for (int n = 0; n < g->cell_count[idx]; ++n) {
+        int s = items[n];
+        float dx = px - cx[s], dy = py - cy[s], dz = pz - cz[s];
+        /* seedSpinsKernel's test (sim3d_kernel.cu:299) */
+        if (dx*dx + dy*dy + dz*dz < rr[s]*rr[s] && (int)sid[s] < label) label = (int)sid[s];
+    }
+    return label;
+}
+
+/*
+ * Rejection seeding (sim3d_kernel.cu:240-337, geometry.py:73-174).  A
+ * position is accepted when the first structure, in id order with the box
+ * last, that contains it is a target; the box counts only strictly inside.
+ * target[k] != 0 marks structure k (k = nstructures is the box) as a target.
+ * Positions are (u - 0.5) * L with Philox uniforms of round r at counter
+ * (walker, r, 0, stream); at most max_rounds rounds.  Returns the number of
+ * walkers left unseeded.
+ */
+OZ_API int oz_seed(const oz_geom* g, const unsigned char* target, int N, uint32_t key0, uint32_t key1,
+                   uint32_t stream, int max_rounds, float* spins, int* label, int nthreads) {
+    const int nt = oz_threads(nthreads);
+    int unseeded = 0;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 256) reduction(+:unseeded)
+    for (int w = 0; w < N; ++w) {
+        int ok = 0;
+        for (int r = 0; r < max_rounds && !ok; ++r) {
+            float u0, u1, u2;
+            oz_philox_uniform3(key0, key1, stream, (uint32_t)w, (uint32_t)r, &u0, &u1, &u2);
+            float px = (u0 - 0.5f) * g->Lx;
+            float py = (u1 - 0.5f) * g->Ly;
+            float pz = (u2 - 0.5f) * g->Lz;
+            int lab = oz_label_of(g, px, py, pz);
+            int accept;
+            if (lab < g->nstructures) accept = target[lab] != 0;
+            else accept = target[g->nstructures] &&
+                          px > -g->Lx/2 && px < g->Lx/2 && py > -g->Ly/2 && py < g->Ly/2 &&
+                          pz > -g->Lz/2 && pz < g->Lz/2;
+            if (accept) {
+                spins[w] = px; spins[N + w] = py; spins[2*N + w] = pz;
+                if (label) label[w] = lab;
+                ok = 1;
+            }
+        }
+        if (!ok) {
+            unseeded++;
+            if (label) label[w] = -1;
+        }
+    }
+    return unseeded;
+}
+
+/* Accept/reject of given positions under the seeding rule (pinned against the
+ * reference's seedSpinsKernel). */
+OZ_API void oz_seed_accept(const oz_geom* g, const unsigned char* target, int N, const float* pos,
+                           unsigned char* accept) {
+    for (int w = 0; w < N; ++w) {
+        float px = pos[w], py = pos[N + w], pz = pos[2*N + w];
+        int lab = oz_label_of(g, px, py, pz);
+        if (lab < g->nstructures) accept[w] = target[lab] != 0;
+        else accept[w] = target[g->nstructures] &&
+                         px > -g->Lx/2 && px < g->Lx/2 && py > -g->Ly/2 && py < g->Ly/2 &&
+                         pz > -g->Lz/2 && pz < g->Lz/2;
+    }
+}
+
+/* Normals of draws [0, ndraw) of every walker at one step: out[w][d][3]. */
+OZ_API void oz_philox_normals(uint32_t key0, uint32_t key1, uint32_t stream, int N, int step, int ndraw,
+                              float* out) {
+    for (int w = 0; w < N; ++w)
+        for (int d = 0; d < ndraw; ++d) {
+            float* o = out + ((size_t)w * ndraw + d) * 3;
+            oz_philox_normal3(key0, key1, stream, (uint32_t)w, (uint32_t)step, (uint32_t)d, o, o + 1, o + 2);
+        }
+}
+
+/* Sums of dx^2 and dx^4 per axis over walkers, in double
+ * (computeDiffusionCoefficientsAndKurtosis, sim3d_kernel.cu:162-238, before
+ * its division by 2tN and N).  out: [sx2, sy2, sz2, sx4, sy4, sz4]. */
+OZ_API void oz_moments(int N, const float* spins, const float* spins0, double* out) {
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int w = 0; w < N; ++w)
+        for (int a = 0; a < 3; ++a) {
+            double d = (double)spins[a*N + w] - (double)spins0[a*N + w];
+            acc[a] += d*d;
+            acc[3 + a] += d*d*d*d;
+        }
+    memcpy(out, acc, sizeof acc);
+}
+
+/*
+ * Signal from the Kahan 3-vector Phi ([6, N]: sums then compensations):
+ * S[d][b] = (1/N) sum_w exp(i * amp[b] * u_d . (Phi_w - comp_w)), in double.
+ */
+OZ_API void oz_signal_phi(int N, const float* phi, const double* dirs, int ndir, const double* amp, int nb,
+                          double* re, double* im) {
+    for (int i = 0; i < ndir * nb; ++i) { re[i] = 0; im[i] = 0; }
+    for (int w = 0; w < N; ++w) {
+        double px = (double)phi[w] - (double)phi[3*N + w];
+        double py = (double)phi[N + w] - (double)phi[4*N + w];
+        double pz = (double)phi[2*N + w] - (double)phi[5*N + w];
+        for (int d = 0; d < ndir; ++d) {
+            double ph = dirs[d]*px + dirs[ndir + d]*py + dirs[2*ndir + d]*pz;
+            for (int b = 0; b < nb; ++b) {
+                re[d*nb + b] += cos(amp[b]*ph);
+                im[d*nb + b] += sin(amp[b]*ph);
+            }
+        }
+    }
+    for (int i = 0; i < ndir * nb; ++i) { re[i] /= N; im[i] /= N; }
+}
+
+/* Signal from a per-direction phase array [ndir, N] (double). */
+OZ_API void oz_signal_phase(int N, const double* phase, int ndir, const double* amp, int nb,
+                            double* re, double* im) {
+    for (int i = 0; i < ndir * nb; ++i) { re[i] = 0; im[i] = 0; }
+    for (int d = 0; d < ndir; ++d)
+        for (int w = 0; w < N; ++w)
+            for (int b = 0; b < nb; ++b) {
+                re[d*nb + b] += cos(amp[b]*phase[(size_t)d*N + w]);
+                im[d*nb + b] += sin(amp[b]*phase[(size_t)d*N + w]);
+            }
+    for (int i = 0; i < ndir * nb; ++i) { re[i] /= N; im[i] /= N; }
+}

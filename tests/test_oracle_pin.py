@@ -1,0 +1,111 @@
+"""The oracle against the reference's own outputs (golden fixtures).
+
+The fixtures were produced by the reference's Python engine and kernel source
+(tests/golden/make_golden.py); the C oracle must reproduce every float bit for
+bit: positions, spins0, T2 signal, phase; the numpy cell-list restatement must
+reproduce DiffSim3d.set_segments exactly; the seeding rule must accept exactly
+the positions seedSpinsKernel accepts.
+"""
+import numpy as np
+import pytest
+
+from tests._fixtures import DWI, NARROW, dirs_of, load, oracle_geometry
+from oracle import oracle as oz
+from oracle.cells_oracle import cells_members, segments_reference
+
+
+@pytest.mark.parametrize("name", NARROW)
+def test_narrow_pulse_bit_exact(name):
+    c = load(name)
+    g = oracle_geometry(c)
+    spins = c["x0"].copy()
+    spins0 = spins.copy()
+    sig = np.ones(int(c["N"]), np.float32)
+    r = oz.walk_f32(g, oz.philox(int(c["key"])), oz.MODE_SIG, spins, spins0, 0, int(c["nt"]), float(c["dt"]),
+                    sig=sig)
+    np.testing.assert_array_equal(spins, c["spins"])
+    np.testing.assert_array_equal(spins0, c["spins0"])
+    # T2 weighting goes through expf (glibc here, the reference's libm there): ulps only
+    np.testing.assert_allclose(sig, c["sig"], rtol=2e-6)
+    assert (r["flags"] & oz.FLAG_DRAWS_EXHAUSTED).sum() == 0
+
+
+@pytest.mark.parametrize("name", DWI)
+def test_dwi_phase_bit_exact(name):
+    c = load(name)
+    g = oracle_geometry(c)
+    N = int(c["N"])
+    dirs = dirs_of(c)
+    spins = c["x0"].astype(np.float32).copy()
+    spins0 = spins.copy()
+    phase = np.zeros((dirs.shape[1], N), np.float32)
+    oz.walk_f32(g, oz.philox(int(c["key"])), oz.MODE_PHASE, spins, spins0, 0, int(c["nt"]), float(c["dt"]),
+                G=c["G"], Garea=c["Garea"], phase=phase, diffdir=dirs)
+    np.testing.assert_array_equal(spins, c["spins"])
+    np.testing.assert_array_equal(spins0, c["spins0"])
+    np.testing.assert_array_equal(phase, c["phase"])
+
+
+def test_three_axis_equals_identity_directions():
+    """randomWalk3d_phase (fixed x, y, z) is randomWalk3d_phase_multidirr with
+    the identity as directions."""
+    c = load("dwi_overlap_3axis")
+    assert c["phase"].shape[0] == 3
+
+
+def test_segments_match_set_segments():
+    z = np.load(__import__("tests._fixtures", fromlist=["GOLDEN"]).GOLDEN / "segments.npz")
+    for i in range(int(z["ncase"])):
+        K, seg = segments_reference(z[f"case{i}_spheres"], tuple(z[f"case{i}_L"]), tuple(z[f"case{i}_nseg"]))
+        assert K == int(z[f"case{i}_K"])
+        np.testing.assert_array_equal(seg, z[f"case{i}_segments"])
+    for name in NARROW + DWI:
+        c = load(name)
+        nseg = tuple(int(v) for v in c["nseg"])
+        K, seg = segments_reference(c["spheres"], tuple(c["L"]), nseg)
+        assert K == int(c["K"])
+        _assert_same_up_to_ties(c["spheres"], tuple(c["L"]), nseg, K, seg, c["segments"])
+
+
+def _assert_same_up_to_ties(spheres, L, nseg, K, mine, ref):
+    """The reference's unstable argsort may pick a different pad among spheres
+    with equal in_segment; members must agree and pads must tie."""
+    from oracle.cells_oracle import in_segment
+    nx, ny, nz = nseg
+    mine, ref = mine.reshape(-1, K), ref.reshape(-1, K)
+    for n in range(nx):
+        for m in range(ny):
+            for p in range(nz):
+                c = p * nx * ny + m * nx + n
+                v = in_segment(spheres, L, nseg, (n, m, p))
+                members = set(np.nonzero(v < 1.0)[0])
+                assert members <= set(mine[c]) and members <= set(ref[c])
+                np.testing.assert_array_equal(np.sort(v[mine[c]]), np.sort(v[ref[c]]))
+
+
+def test_members_are_subset_of_padded_lists():
+    z = np.load(__import__("tests._fixtures", fromlist=["GOLDEN"]).GOLDEN / "segments.npz")
+    for i in range(int(z["ncase"])):
+        nseg = tuple(int(v) for v in z[f"case{i}_nseg"])
+        st, ct, it = cells_members(z[f"case{i}_spheres"], tuple(z[f"case{i}_L"]), nseg)
+        K = int(z[f"case{i}_K"])
+        assert ct.max() == K
+        seg = z[f"case{i}_segments"].reshape(-1, K)
+        for c in range(seg.shape[0]):
+            assert set(it[st[c]:st[c] + ct[c]]) <= set(seg[c])
+
+
+def test_seeding_rule_matches_seedSpinsKernel():
+    from tests._fixtures import GOLDEN
+    z = np.load(GOLDEN / "seeding.npz")
+    L = tuple(z["L"])
+    sph = z["spheres"]
+    st, ct, it = cells_members(sph, L, (1, 1, 1))
+    g = oz.Geometry(sph.astype(np.float32), 3, L, (1, 1, 1), st, ct, it, np.full(4, 2.0, np.float32),
+                    np.full(4, 100.0, np.float32))
+    u = z["u"]
+    pos = ((u.T - np.float32(0.5)) * np.array(L, np.float32)[:, None]).astype(np.float32)
+    for t in ("intra", "extra", "s1", "all"):
+        acc = oz.seed_accept(g, z[f"{t}_targets"], pos)
+        np.testing.assert_array_equal(acc, z[f"{t}_accept"])
+        np.testing.assert_array_equal(pos[:, acc], z[f"{t}_pos"][:, acc])
