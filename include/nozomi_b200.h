@@ -1,0 +1,223 @@
+/*
+ * nozomi_b200 — C ABI of the B200 spin random-walk library (libnozomi_b200.so).
+ *
+ * Every entry point takes device pointers, sizes and a cudaStream_t (passed as
+ * void*, NULL = legacy default stream), enqueues its kernels on that stream and
+ * returns a status: NZ_OK or an error code; nz_last_error() gives the message of
+ * the calling thread's last failure.  No entry point allocates device memory or
+ * synchronises the stream unless its comment says so; scratch buffers are
+ * passed in by the caller.
+ *
+ * Each declaration names the reference interface it replaces (paths relative to
+ * the nozomi source tree, simulation_toolkit/simulation_engine/...).  The
+ * reference has no C ABI: its boundary is the Python object API of
+ * DiffSim3d / DwiSim3d driving pycuda kernels, so the cited lines are those
+ * methods and kernels.
+ */
+#ifndef NOZOMI_B200_H
+#define NOZOMI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NZ_VERSION 1
+
+/* status codes */
+#define NZ_OK 0
+#define NZ_ERR_ARG 1        /* invalid argument (message in nz_last_error) */
+#define NZ_ERR_CUDA 2       /* a CUDA launch or runtime call failed */
+#define NZ_ERR_CAPACITY 3   /* a caller-provided buffer is too small */
+#define NZ_ERR_UNSEEDED 4   /* seeding left walkers unplaced after its round limit */
+
+/* walk modes (bit set) */
+#define NZ_MODE_SIG 1       /* T2 weighting of sig[] (randomWalk3d) */
+#define NZ_MODE_PHASE 2     /* per-direction phase[ndir][N] (randomWalk3d_phase_multidirr) */
+#define NZ_MODE_PHI 4       /* Kahan 3-vector Phi = sum_n G_n p_n; phase_d = u_d . Phi */
+#define NZ_MODE_MOMENTS 8   /* per-step displacement moments (fused walk only) */
+
+/* per-walker flag bits */
+#define NZ_FLAG_DRAWS_EXHAUSTED 1
+#define NZ_FLAG_ITER_CAP 2
+#define NZ_FLAG_UNSEEDED 4
+
+/* Box [-L/2, L/2]^3 and uniform cell grid: the reference kernel's template
+ * constants Lx..Lz, dLx..dLz, nLx..nLz (sim3d_kernel.cu:17-28). */
+typedef struct nz_grid {
+    float Lx, Ly, Lz;
+    float dLx, dLy, dLz;
+    int nx, ny, nz;
+} nz_grid;
+
+/* A substrate on the device: spheres in the reference's SoA layout
+ * (geometry.py:58-64, [5,S] = cx, cy, cz, r, structure id), compact cell lists
+ * and the per-structure D and T2 (structure nstructures is the box,
+ * diffsim3d.py:95-103). */
+typedef struct nz_substrate {
+    nz_grid grid;
+    int nstructures;
+    int S;
+    const float* spheres;      /* [5, S] float32 */
+    const int* cell_start;     /* [ncell] offset of each cell's list in cell_items */
+    const int* cell_count;     /* [ncell] */
+    const int* cell_items;     /* sphere indices, ascending within a cell */
+    const float* cell_sph4;    /* [n_items][4] cx, cy, cz, r of each list entry (fused walk) */
+    const int* cell_sid;       /* [n_items] structure id of each list entry (fused walk) */
+    const float* D;            /* [nstructures + 1] um^2/ms */
+    const float* T2;           /* [nstructures + 1] ms */
+} nz_substrate;
+
+/* Source of the normal draws: an injected table normals[N][nsteps][maxk]
+ * (k-th normal of a walker within a step; the reference's draw order), or,
+ * with table == NULL, Philox4x32-10 at counter (walker, step, draw, stream)
+ * under key (key0, key1). */
+typedef struct nz_draws {
+    const float* table;
+    int nsteps, maxk;
+    uint32_t key0, key1, stream;
+} nz_draws;
+
+/* Walkers in the reference's layout (diffsim3d.py:42-45, :62). */
+typedef struct nz_walkers {
+    int N;
+    float* spins;          /* [3, N] */
+    float* spins0;         /* [3, N] */
+    float* phase;          /* [ndir, N] (NZ_MODE_PHASE) */
+    const float* diffdir;  /* [3, ndir] (NZ_MODE_PHASE) */
+    int ndir;
+    float* sig;            /* [N] (NZ_MODE_SIG) */
+    float* phi;            /* [6, N] Phi sums then compensations (NZ_MODE_PHI) */
+    int* label;            /* [N] structure of the walker at its last iteration, or NULL */
+    int* n_iter;           /* [N] accumulated collision-loop iterations, or NULL */
+    int* n_scatter;        /* [N] accumulated scatterings (truncated jumps), or NULL */
+    int* flags;            /* [N] NZ_FLAG_* bits, or NULL */
+} nz_walkers;
+
+/* Walkers packed for the fused walk: four float4 per walker,
+ * pos = (x, y, z, label bits), org = (x0, y0, z0, walker id bits),
+ * phi = (Phi_x, Phi_y, Phi_z, sig), comp = (Kahan x, y, z, flag bits). */
+typedef struct nz_state {
+    int N;
+    float* pos;
+    float* org;
+    float* phi;
+    float* comp;
+} nz_state;
+
+/* One job of the batched walk: a substrate, a protocol and a walker range. */
+typedef struct nz_job {
+    nz_substrate sub;
+    const float* G;        /* [nsteps] unit-waveform phase increment per step */
+    const float* Garea;    /* [nsteps] wrap correction per step */
+    int nsteps;
+    float dt;
+    nz_draws draws;        /* Philox only (table must be NULL) */
+    int mode;              /* NZ_MODE_PHI and/or NZ_MODE_SIG */
+    nz_state state;
+    double* moments;       /* [nsteps][6] (NZ_MODE_MOMENTS) or NULL */
+} nz_job;
+
+/* A work item: walkers [first, first + count) of job `job`, count <= block size. */
+typedef struct nz_item {
+    int job;
+    int first;
+    int count;
+} nz_item;
+
+int nz_version(void);
+const char* nz_status_string(int status);
+const char* nz_last_error(void);
+int nz_device_sm_count(int* sms);
+
+/* ---- a1: cell lists — DiffSim3d.set_segments (diffsim3d.py:107-174) ---- */
+
+/* Number of member spheres of every cell: in_segment < jump_tol, evaluated in
+ * float64 in the reference's operation order (diffsim3d.py:128-141).
+ * spheres64: [5, S] float64. counts: [nx*ny*nz]. */
+int nz_cells_count(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz,
+                   double jump_tol, int* counts, void* stream);
+
+/* Exclusive prefix sum of n ints (one block; n <= 1<<26); total receives the sum. */
+int nz_exclusive_scan_i32(const int* in, int* out, int n, int* total, void* stream);
+
+/* Member lists: items[offsets[c] ...] gets the counts[c] members of cell c in
+ * ascending index order.  offsets = exclusive scan of counts (nz_cells_count);
+ * cursor: scratch of nx*ny*nz ints. */
+int nz_cells_fill(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz,
+                  double jump_tol, const int* offsets, const int* counts, int* cursor, int* items, void* stream);
+
+/* The reference's padded table (diffsim3d.py:144-168): K = the largest member
+ * count; cell c's K entries at segments[c*K] are the K spheres of smallest
+ * in_segment (ties by lower index), ascending by index. */
+int nz_segments_fill(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz,
+                     int K, int* segments, void* stream);
+
+/* Denormalised list entries for the fused walk: sph4[k] = (cx, cy, cz, r) and
+ * sid[k] = structure id of sphere items[k]. */
+int nz_cells_gather(const float* spheres, int S, const int* items, int n_items, float* sph4, int* sid,
+                    void* stream);
+
+/* ---- a7: seeding — seedSpinsKernel (sim3d_kernel.cu:240-337) + SimGeometry3D.gpu_seed
+ * (geometry.py:73-174).  target[k] != 0 marks structure k (k = nstructures is the
+ * box) as a target.  A position is accepted when the first structure in id order
+ * containing it is a target (the box only strictly inside).  Round r draws
+ * Philox uniforms at (walker, r, 0, stream); at most max_rounds rounds, all in one
+ * launch (no host round trips).  spins: [3,N]; label: [N] (-1 = unseeded);
+ * n_unseeded: one device int.  Returns NZ_OK; check *n_unseeded on the host. */
+int nz_seed(const nz_substrate* sub, const uint8_t* target, int N, uint32_t key0, uint32_t key1,
+            uint32_t stream_id, int max_rounds, float* spins, int* label, int* n_unseeded, void* stream);
+
+/* ---- a3/a4/a5: one time step of every walker, one launch —
+ * randomWalk3d (sim3d_kernel.cu:340-522), randomWalk3d_phase (:524-717),
+ * randomWalk3d_phase_multidirr (:719-943) as launched by DiffSim3d.step /
+ * dwi_step / dwi_multidirections_step (diffsim3d.py:199-226). */
+int nz_walk_step(const nz_substrate* sub, const nz_walkers* wk, int mode, float dt, float G, float Garea,
+                 int step, const nz_draws* draws, void* stream);
+
+/* ---- fused walk: steps [step0, step1) of every walker in one launch, state
+ * in registers, G/Garea tables on the device (DwiSim3d.simulate_multi_directions'
+ * loop, diffsim3d.py:246-261, moved onto the device). ---- */
+int nz_state_pack(const nz_walkers* wk, const uint32_t* walker_id, nz_state* st, void* stream);
+int nz_state_unpack(const nz_state* st, const nz_walkers* wk, void* stream);
+
+int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mode, float dt, const float* G,
+                  const float* Garea, int step0, int step1, const nz_draws* draws, double* moments,
+                  void* stream);
+
+/* ---- batched persistent walk: every item of every job, steps [step0, step1)
+ * of each job (clamped to its nsteps), CTAs pulling items from *queue (one
+ * device int, zeroed by the caller) until none is left.  jobs and items are
+ * device arrays; every job of one launch has mode `mode`.  grid = CTA count
+ * (0 = one CTA per item, no queue).  Items hold at most 128 walkers. ---- */
+int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0, int step1,
+                  int* queue, int grid, void* stream);
+
+/* ---- walker re-binning: a stable-key counting sort of the packed state by
+ * cell, so that the walkers of one CTA share cells.  bins: bin per walker is
+ * the cell of its position under `grid` coarsened by `coarsen` per axis;
+ * scratch: nz_sort_scratch_bytes(N, nbins) bytes; out: a second state. ---- */
+size_t nz_sort_scratch_bytes(int N, int nbins);
+int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out, void* scratch,
+                  size_t scratch_bytes, void* stream);
+
+/* ---- a13: signal S[d][b] = sum_w exp(i * amp[b] * u_d . Phi_w) over walkers,
+ * FP32 per walker, FP64 sums (the reference stops at per-spin phase,
+ * diffsim3d.py:257-261).  dirs: [3, ndir]; amp: [nb]; out: [2][ndir][nb] doubles
+ * (real then imaginary), accumulated into (zero it first). ---- */
+int nz_signal_phi(const nz_state* st, const float* dirs, int ndir, const float* amp, int nb, double* out,
+                  void* stream);
+
+/* Per-direction phase from Phi: phase[d][w] = u_d . (Phi_w - comp_w), float. */
+int nz_phase_from_phi(const nz_state* st, const float* dirs, int ndir, float* phase, void* stream);
+
+/* ---- a8: displacement moments of one step —
+ * computeDiffusionCoefficientsAndKurtosis (sim3d_kernel.cu:162-238) before its
+ * divisions: out[6] += (sum dx^2, dy^2, dz^2, dx^4, dy^4, dz^4), FP64. ---- */
+int nz_moments(const float* spins, const float* spins0, int N, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NOZOMI_B200_H */

@@ -1,0 +1,113 @@
+"""ctypes binding of libnozomi_b200.so (the C ABI declared in include/nozomi_b200.h).
+
+The library is the only compute path: loading fails loudly when it is missing
+or when no CUDA device is present; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libnozomi_b200.so"
+
+NZ_OK, NZ_ERR_ARG, NZ_ERR_CUDA, NZ_ERR_CAPACITY, NZ_ERR_UNSEEDED = 0, 1, 2, 3, 4
+MODE_SIG, MODE_PHASE, MODE_PHI, MODE_MOMENTS = 1, 2, 4, 8
+FLAG_DRAWS_EXHAUSTED, FLAG_ITER_CAP, FLAG_UNSEEDED = 1, 2, 4
+FUSED_THREADS = 128       # walkers per CTA / per work item of the fused and batched walks
+MOMENT_STEPS = 256        # steps per launch when the fused walk accumulates moments
+
+_P = ctypes.c_void_p
+_i = ctypes.c_int
+_f = ctypes.c_float
+_d = ctypes.c_double
+_u = ctypes.c_uint32
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("Lx", _f), ("Ly", _f), ("Lz", _f), ("dLx", _f), ("dLy", _f), ("dLz", _f),
+                ("nx", _i), ("ny", _i), ("nz", _i)]
+
+
+class Substrate(ctypes.Structure):
+    _fields_ = [("grid", Grid), ("nstructures", _i), ("S", _i), ("spheres", _P), ("cell_start", _P),
+                ("cell_count", _P), ("cell_items", _P), ("cell_sph4", _P), ("cell_sid", _P), ("D", _P),
+                ("T2", _P)]
+
+
+class Draws(ctypes.Structure):
+    _fields_ = [("table", _P), ("nsteps", _i), ("maxk", _i), ("key0", _u), ("key1", _u), ("stream", _u)]
+
+
+class Walkers(ctypes.Structure):
+    _fields_ = [("N", _i), ("spins", _P), ("spins0", _P), ("phase", _P), ("diffdir", _P), ("ndir", _i),
+                ("sig", _P), ("phi", _P), ("label", _P), ("n_iter", _P), ("n_scatter", _P), ("flags", _P)]
+
+
+class State(ctypes.Structure):
+    _fields_ = [("N", _i), ("pos", _P), ("org", _P), ("phi", _P), ("comp", _P)]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("sub", Substrate), ("G", _P), ("Garea", _P), ("nsteps", _i), ("dt", _f), ("draws", Draws),
+                ("mode", _i), ("state", State), ("moments", _P)]
+
+
+class Item(ctypes.Structure):
+    _fields_ = [("job", _i), ("first", _i), ("count", _i)]
+
+
+# name -> (restype, argtypes); every symbol of include/nozomi_b200.h
+SIGNATURES = {
+    "nz_version": (_i, []),
+    "nz_status_string": (ctypes.c_char_p, [_i]),
+    "nz_last_error": (ctypes.c_char_p, []),
+    "nz_device_sm_count": (_i, [_P]),
+    "nz_cells_count": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _d, _P, _P]),
+    "nz_exclusive_scan_i32": (_i, [_P, _P, _i, _P, _P]),
+    "nz_cells_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _d, _P, _P, _P, _P, _P]),
+    "nz_segments_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _i, _P, _P]),
+    "nz_cells_gather": (_i, [_P, _i, _P, _i, _P, _P, _P]),
+    "nz_seed": (_i, [_P, _P, _i, _u, _u, _u, _i, _P, _P, _P, _P]),
+    "nz_walk_step": (_i, [_P, _P, _i, _f, _f, _f, _i, _P, _P]),
+    "nz_state_pack": (_i, [_P, _P, _P, _P]),
+    "nz_state_unpack": (_i, [_P, _P, _P]),
+    "nz_walk_fused": (_i, [_P, _P, _i, _f, _P, _P, _i, _i, _P, _P, _P]),
+    "nz_walk_batch": (_i, [_P, _i, _P, _i, _i, _i, _i, _P, _i, _P]),
+    "nz_sort_scratch_bytes": (ctypes.c_size_t, [_i, _i]),
+    "nz_state_sort": (_i, [_P, _P, _i, _P, _P, ctypes.c_size_t, _P]),
+    "nz_signal_phi": (_i, [_P, _P, _i, _P, _i, _P, _P]),
+    "nz_phase_from_phi": (_i, [_P, _P, _i, _P, _P]),
+    "nz_moments": (_i, [_P, _P, _i, _P, _P]),
+}
+
+_lib = None
+
+
+class NozomiError(RuntimeError):
+    pass
+
+
+def load(require_built: bool = True) -> ctypes.CDLL:
+    """Load the library (no GPU needed to load it)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise NozomiError(f"{LIB_PATH} is missing: build it with `python -m nozomi_b200.build`")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(rc: int, what: str = ""):
+    if rc != NZ_OK:
+        lib = load()
+        msg = lib.nz_last_error().decode(errors="replace")
+        raise NozomiError(f"{what or 'nozomi_b200'}: {lib.nz_status_string(rc).decode()} ({msg})")
+
+
+def byref(s):
+    return ctypes.byref(s)

@@ -1,0 +1,178 @@
+// C entry points of libnozomi_b200.so that are not next to their kernels:
+// status handling, the plain step, packing and the fused / batched walks.
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include "kernels.cuh"
+
+namespace nz {
+
+static thread_local char g_last_error[512] = "";
+
+int set_error(int status, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof g_last_error, fmt, ap);
+  va_end(ap);
+  return status;
+}
+
+int check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(NZ_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return NZ_OK;
+}
+
+static Grid to_grid(const nz_grid& g) {
+  return Grid{g.Lx, g.Ly, g.Lz, g.dLx, g.dLy, g.dLz, float(g.nx), float(g.ny), float(g.nz)};
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace nz
+
+using namespace nz;
+
+extern "C" int nz_version(void) { return NZ_VERSION; }
+
+extern "C" const char* nz_status_string(int status) {
+  switch (status) {
+    case NZ_OK: return "ok";
+    case NZ_ERR_ARG: return "invalid argument";
+    case NZ_ERR_CUDA: return "CUDA error";
+    case NZ_ERR_CAPACITY: return "buffer too small";
+    case NZ_ERR_UNSEEDED: return "walkers left unseeded";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char* nz_last_error(void) { return g_last_error; }
+
+extern "C" int nz_device_sm_count(int* sms) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_launch("cudaGetDevice");
+  if (cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return check_launch("cudaDeviceGetAttribute");
+  return NZ_OK;
+}
+
+static int check_substrate(const nz_substrate* s, const char* who) {
+  if (!s) return set_error(NZ_ERR_ARG, "%s: null substrate", who);
+  if (s->grid.nx <= 0 || s->grid.ny <= 0 || s->grid.nz <= 0 || s->nstructures < 0 || s->S < 0 || !s->cell_start ||
+      !s->cell_count || !s->D)
+    return set_error(NZ_ERR_ARG, "%s: incomplete substrate", who);
+  return NZ_OK;
+}
+
+extern "C" int nz_walk_step(const nz_substrate* sub, const nz_walkers* wk, int mode, float dt, float G, float Garea,
+                            int step, const nz_draws* draws, void* stream) {
+  int rc = check_substrate(sub, "nz_walk_step");
+  if (rc) return rc;
+  if (!wk || !draws || wk->N < 0 || !wk->spins || !wk->spins0 || !sub->cell_items || (sub->S > 0 && !sub->spheres))
+    return set_error(NZ_ERR_ARG, "nz_walk_step: bad walkers or draws");
+  if ((mode & NZ_MODE_PHASE) && (wk->ndir <= 0 || !wk->phase || !wk->diffdir))
+    return set_error(NZ_ERR_ARG, "nz_walk_step: phase mode needs phase and diffdir");
+  if ((mode & NZ_MODE_SIG) && (!wk->sig || !sub->T2)) return set_error(NZ_ERR_ARG, "nz_walk_step: sig mode needs sig, T2");
+  if ((mode & NZ_MODE_PHI) && !wk->phi) return set_error(NZ_ERR_ARG, "nz_walk_step: phi mode needs phi");
+  if (mode & ~(NZ_MODE_SIG | NZ_MODE_PHASE | NZ_MODE_PHI)) return set_error(NZ_ERR_ARG, "nz_walk_step: mode %d", mode);
+  if (wk->N == 0) return NZ_OK;
+  PlainArgs a;
+  a.g = to_grid(sub->grid);
+  a.nstructures = sub->nstructures;
+  a.S = sub->S;
+  a.N = wk->N;
+  a.spheres = sub->spheres;
+  a.cell_start = sub->cell_start;
+  a.cell_count = sub->cell_count;
+  a.cell_items = sub->cell_items;
+  a.D = sub->D;
+  a.T2 = sub->T2;
+  a.spins = wk->spins;
+  a.spins0 = wk->spins0;
+  a.phase = wk->phase;
+  a.diffdir = wk->diffdir;
+  a.ndir = wk->ndir;
+  a.sig = wk->sig;
+  a.phi = wk->phi;
+  a.dt = dt;
+  a.G = G;
+  a.Garea = Garea;
+  a.step = step;
+  a.draws = Draws{draws->table, draws->nsteps, draws->maxk, draws->key0, draws->key1, draws->stream};
+  a.mode = mode;
+  a.label = wk->label;
+  a.n_iter = wk->n_iter;
+  a.n_scatter = wk->n_scatter;
+  a.flags = wk->flags;
+  walk_plain_kernel<<<(wk->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  return check_launch("walk_plain_kernel");
+}
+
+static int check_state(const nz_state* st, const char* who) {
+  if (!st || st->N < 0 || !st->pos || !st->org || !st->phi || !st->comp)
+    return set_error(NZ_ERR_ARG, "%s: incomplete state", who);
+  if (!aligned16(st->pos) || !aligned16(st->org) || !aligned16(st->phi) || !aligned16(st->comp))
+    return set_error(NZ_ERR_ARG, "%s: state arrays must be 16-byte aligned", who);
+  return NZ_OK;
+}
+
+extern "C" int nz_state_pack(const nz_walkers* wk, const uint32_t* walker_id, nz_state* st, void* stream) {
+  int rc = check_state(st, "nz_state_pack");
+  if (rc) return rc;
+  if (!wk || wk->N != st->N || !wk->spins || !wk->spins0) return set_error(NZ_ERR_ARG, "nz_state_pack: bad walkers");
+  if (st->N == 0) return NZ_OK;
+  pack_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*wk, walker_id, *st);
+  return check_launch("pack_kernel");
+}
+
+extern "C" int nz_state_unpack(const nz_state* st, const nz_walkers* wk, void* stream) {
+  int rc = check_state(st, "nz_state_unpack");
+  if (rc) return rc;
+  if (!wk || wk->N != st->N || !wk->spins || !wk->spins0) return set_error(NZ_ERR_ARG, "nz_state_unpack: bad walkers");
+  if (st->N == 0) return NZ_OK;
+  unpack_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*st, *wk);
+  return check_launch("unpack_kernel");
+}
+
+static int check_fused_sub(const nz_substrate* sub, const char* who) {
+  int rc = check_substrate(sub, who);
+  if (rc) return rc;
+  if (!sub->cell_sph4 || !sub->cell_sid) return set_error(NZ_ERR_ARG, "%s: substrate lacks cell_sph4/cell_sid", who);
+  if (!aligned16(sub->cell_sph4)) return set_error(NZ_ERR_ARG, "%s: cell_sph4 must be 16-byte aligned", who);
+  return NZ_OK;
+}
+
+extern "C" int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mode, float dt, const float* G,
+                             const float* Garea, int step0, int step1, const nz_draws* draws, double* moments,
+                             void* stream) {
+  int rc = check_fused_sub(sub, "nz_walk_fused");
+  if (rc) return rc;
+  rc = check_state(st, "nz_walk_fused");
+  if (rc) return rc;
+  if (!draws || draws->table) return set_error(NZ_ERR_ARG, "nz_walk_fused: Philox draws only (table must be NULL)");
+  if ((mode & NZ_MODE_PHI) && (!G || !Garea)) return set_error(NZ_ERR_ARG, "nz_walk_fused: phi mode needs G, Garea");
+  if ((mode & NZ_MODE_SIG) && !sub->T2) return set_error(NZ_ERR_ARG, "nz_walk_fused: sig mode needs T2");
+  if (mode & NZ_MODE_MOMENTS) {
+    if (!moments) return set_error(NZ_ERR_ARG, "nz_walk_fused: moments mode needs moments");
+    if (step1 - step0 > kMomentSteps)
+      return set_error(NZ_ERR_ARG, "nz_walk_fused: moments mode runs at most %d steps per launch", kMomentSteps);
+  }
+  if (step0 < 0 || step1 < step0) return set_error(NZ_ERR_ARG, "nz_walk_fused: bad step range");
+  if (st->N == 0 || step1 == step0) return NZ_OK;
+  const JobDev j = make_job(*sub, G, Garea, step1, dt, *draws, mode, *st, moments);
+  const int n_items = (st->N + kFusedThreads - 1) / kFusedThreads;
+  return launch_fused(mode, j, nullptr, nullptr, n_items, step0, step1, nullptr, n_items,
+                      static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0,
+                             int step1, int* queue, int grid, void* stream) {
+  if (!jobs || n_jobs <= 0 || !items || n_items < 0 || step0 < 0 || step1 < step0 || grid < 0)
+    return set_error(NZ_ERR_ARG, "nz_walk_batch: bad arguments");
+  if (grid > 0 && !queue) return set_error(NZ_ERR_ARG, "nz_walk_batch: a persistent grid needs a queue counter");
+  if (mode & NZ_MODE_MOMENTS) return set_error(NZ_ERR_ARG, "nz_walk_batch: moments are per-substrate (nz_walk_fused)");
+  if (n_items == 0 || step1 == step0) return NZ_OK;
+  const JobDev unused{};
+  return launch_fused(mode, unused, jobs, items, n_items, step0, step1, grid > 0 ? queue : nullptr,
+                      grid > 0 ? grid : n_items, static_cast<cudaStream_t>(stream));
+}

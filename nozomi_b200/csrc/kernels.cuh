@@ -1,0 +1,77 @@
+// Structures shared between the kernel files and the C entry points.
+#pragma once
+#include <cstdint>
+#include "nozomi_b200.h"
+#include "nz_common.cuh"
+
+namespace nz {
+
+int set_error(int status, const char* fmt, ...);
+int check_launch(const char* what);
+
+// ---- plain walk (walk_plain.cu) ----
+struct PlainArgs {
+  Grid g;
+  int nstructures, S, N;
+  const float* spheres;  // [5, S]: cx, cy, cz, r, structure id
+  const int* cell_start;
+  const int* cell_count;
+  const int* cell_items;
+  const float* D;        // [nstructures + 1]
+  const float* T2;       // [nstructures + 1]
+  float* spins;          // [3, N]
+  float* spins0;         // [3, N]
+  float* phase;          // [ndir, N]
+  const float* diffdir;  // [3, ndir]
+  int ndir;
+  float* sig;            // [N]
+  float* phi;            // [6, N]: Phi sums then Kahan compensations
+  float dt, G, Garea;
+  int step;
+  Draws draws;
+  int mode;
+  int* label;
+  int* n_iter;
+  int* n_scatter;
+  int* flags;
+};
+__global__ void walk_plain_kernel(const PlainArgs a);
+
+// ---- fused walk (walk_fused.cu) ----
+constexpr int kFusedThreads = 128;
+constexpr int kMomentSteps = 256;  // steps per launch in NZ_MODE_MOMENTS (shared-memory staging)
+
+struct JobDev {
+  Grid g;
+  int nstructures;
+  const float4* sph4;
+  const int* sid;
+  const int* cell_start;
+  const int* cell_count;
+  const float* D;
+  const float* T2;
+  const float* G;
+  const float* Garea;
+  int nsteps;
+  float dt;
+  uint32_t key0, key1, stream;
+  int mode;
+  float4* pos;
+  float4* org;
+  float4* phi;
+  float4* comp;
+  double* moments;
+  int nwalkers;
+};
+
+__host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, const float* Garea, int nsteps, float dt,
+                                    const nz_draws& d, int mode, const nz_state& st, double* moments);
+int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
+                 int step1, int* queue, int grid, cudaStream_t st);
+__global__ void pack_kernel(nz_walkers wk, const uint32_t* ids, nz_state st);
+__global__ void unpack_kernel(nz_state st, nz_walkers wk);
+
+// ---- cells.cu ----
+__global__ void scan_kernel(const int* __restrict__ in, int* __restrict__ out, int n, int* __restrict__ total);
+
+}  // namespace nz

@@ -1,0 +1,370 @@
+// Fused walk: many time steps per launch, walker state in registers.
+//
+// The collision rule is the reference's, unchanged
+// (simulation_toolkit/simulation_engine/sim3d_kernel.cu:758-874): label, first
+// draw, collision pass over the cell's spheres, advance, scatter or continue.
+// What changes is how the work is organised:
+//
+//  * one thread per walker runs a whole range of steps; each lane moves to its
+//    next step as soon as its current one ends, so lanes of a warp do not wait
+//    for each other's extra collision iterations at every step;
+//  * the reference's two passes over the cell list (label, then collisions)
+//    are one pass under the label carried from the previous iteration; the
+//    pass proves that label (some containing sphere of that structure, none of
+//    a lower one) or the iteration is redone with the recomputed label, so the
+//    result is the reference's;
+//  * a sphere whose (r + tol) ball lies more than 2 % + 2 nm beyond this
+//    iteration's reach |j| * jump_remaining cannot lower the jump fraction
+//    (its root exceeds jump_remaining), so its quadratic is skipped; the
+//    remaining candidates are collected in a 32-bit mask per 32-sphere chunk
+//    and solved afterwards, so a warp pays for the most candidates of any lane
+//    rather than for the union of all lanes' candidates;
+//  * the cell list entries carry their sphere's (cx, cy, cz, r) and structure
+//    id inline (one 16-byte and one 4-byte read-only load per entry);
+//  * phase is accrued as the 3-vector Phi = sum_n G_n p_n with Kahan
+//    compensation, the wrap correction on the wrapped axis only; every
+//    direction's phase is u_d . Phi (the reference's per-direction sums
+//    regrouped; identical in exact arithmetic);
+//  * draws are counter-based (Philox at walker, step, draw), so a walker's
+//    trajectory does not depend on which thread, CTA or launch runs it.
+#include <cstdint>
+#include "kernels.cuh"
+
+namespace nz {
+
+struct ScanOut {
+  float fin, fout;
+  bool any_in;
+};
+
+// One pass over a cell's list under assumed label L.  Returns false when the
+// walker's label is not L (then nothing in `o` is used).
+__device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const int* __restrict__ sid, int start,
+                                          int count, int nstructures, float x, float y, float z, int L, float a,
+                                          float jx, float jy, float jz, float reach, ScanOut& o) {
+  o.fin = 0.0f;
+  o.fout = kBig;
+  o.any_in = false;
+  bool found = false, lower = false;
+  const float slack = kTol + reach * 1.02f + 2e-3f;
+  for (int base = 0; base < count; base += 32) {
+    const int m = min(32, count - base);
+    uint32_t in_mask = 0u, out_mask = 0u;
+    for (int i = 0; i < m; ++i) {
+      const int k = start + base + i;
+      const int s = __ldg(sid + k);
+      if (s > L) continue;
+      const float4 c = __ldg(sph4 + k);
+      const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
+      const float d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 - c.w * c.w < 0) {
+        in_mask |= 1u << i;
+        if (s < L) lower = true;
+        else found = true;
+      } else if (s < L) {
+        const float t = c.w + slack;
+        if (d2 <= t * t) out_mask |= 1u << i;
+      }
+    }
+    uint32_t todo = in_mask | out_mask;
+    while (todo) {
+      const int i = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int k = start + base + i;
+      const float4 c = __ldg(sph4 + k);
+      const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
+      if (in_mask & (1u << i)) {
+        o.any_in = true;
+        const float f = step_in(dx, dy, dz, c.w, a, jx, jy, jz);
+        if (o.fin < f) o.fin = f;
+      } else {
+        const float f = step_out(dx, dy, dz, c.w, a, jx, jy, jz);
+        if (f < o.fout) o.fout = f;
+      }
+    }
+  }
+  return !(lower || (L < nstructures && !found));
+}
+
+// The reference's label pass (sim3d_kernel.cu:766-785): lowest structure id
+// among the spheres containing the walker, nstructures if none.
+__device__ __forceinline__ int label_of(const float4* __restrict__ sph4, const int* __restrict__ sid, int start,
+                                        int count, int nstructures, float x, float y, float z) {
+  int L = nstructures;
+  for (int i = 0; i < count; ++i) {
+    const int s = __ldg(sid + start + i);
+    if (s < L) {
+      const float4 c = __ldg(sph4 + start + i);
+      if (inside_test(x - c.x, y - c.y, z - c.z, c.w) < 0) L = s;
+    }
+  }
+  return L;
+}
+
+template <int MODE>
+__device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1, float* s_mom) {
+  float4 P = J.pos[w];
+  float4 O = J.org[w];
+  float4 F = make_float4(0.f, 0.f, 0.f, 1.f), C = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (MODE & (NZ_MODE_PHI | NZ_MODE_SIG)) F = J.phi[w];
+  C = J.comp[w];
+  float x = P.x, y = P.y, z = P.z;
+  int label = __float_as_int(P.w);
+  float x0 = O.x, y0 = O.y, z0 = O.z;
+  const uint32_t wid = __float_as_uint(O.w);
+  float fx = F.x, fy = F.y, fz = F.z, sig = F.w;
+  float kx = C.x, ky = C.y, kz = C.z;
+  int flags = __float_as_int(C.w);
+  if (label < 0 || label > J.nstructures) label = J.nstructures;
+
+  const float dt = J.dt;
+  int s = s0;
+  int niter = 0, draw = 0, start = 0, count = 0;
+  float jr = 1.0f, ds = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+  float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
+  while (s < s1) {
+    if (niter == 0) {
+      const int cell = cell_of(J.g, x, y, z);
+      start = __ldg(J.cell_start + cell);
+      count = __ldg(J.cell_count + cell);
+      jr = 1.0f;
+      draw = 0;
+    }
+    niter++;
+    float jc = jr;
+    if (niter == 1) {
+      philox_normal3(J.key0, J.key1, J.stream, wid, uint32_t(s), 0u, n0, n1, n2);
+      draw = 1;
+      ds = sqrtf(2 * __ldg(J.D + label) * dt);
+      jx = ds * n0;
+      jy = ds * n1;
+      jz = ds * n2;
+    }
+    float a = jx * jx + jy * jy + jz * jz;
+    ScanOut r;
+    if (!scan_cell(J.sph4, J.sid, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, sqrtf(a) * jr, r)) {
+      label = label_of(J.sph4, J.sid, start, count, J.nstructures, x, y, z);
+      if (niter == 1) {
+        ds = sqrtf(2 * __ldg(J.D + label) * dt);
+        jx = ds * n0;
+        jy = ds * n1;
+        jz = ds * n2;
+        a = jx * jx + jy * jy + jz * jz;
+      }
+      scan_cell(J.sph4, J.sid, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, sqrtf(a) * jr, r);
+    }
+    jc = ref_min(jc, r.any_in ? r.fin : kBig);
+    jc = ref_min(jc, r.fout);
+    x += jc * jx;
+    y += jc * jy;
+    z += jc * jz;
+    if (jc < jr) {
+      jr = sqrtf(ref_max(0, jr * jr - jc * jc));
+      if (MODE & NZ_MODE_SIG) sig *= t2_decay(-jc * jc * dt / __ldg(J.T2 + label));
+      philox_normal3(J.key0, J.key1, J.stream, wid, uint32_t(s), uint32_t(draw), n0, n1, n2);
+      draw++;
+      jx = ds * n0;
+      jy = ds * n1;
+      jz = ds * n2;
+    } else {
+      jr -= jc;
+      if (MODE & NZ_MODE_SIG) sig *= t2_decay(-jc * dt / __ldg(J.T2 + label));
+    }
+    if (!((jr > kTol) && (niter < kMaxIter))) {
+      if (niter >= kMaxIter && jr > kTol) flags |= kFlagIterCap;
+      if (MODE & NZ_MODE_PHI) {
+        const float G = __ldg(J.G + s);
+        kahan_add(fx, kx, G * x);
+        kahan_add(fy, ky, G * y);
+        kahan_add(fz, kz, G * z);
+      }
+      const float Ga = (MODE & NZ_MODE_PHI) ? __ldg(J.Garea + s) : 0.0f;
+      const float Lx = J.g.Lx, Ly = J.g.Ly, Lz = J.g.Lz;
+      if (x < -Lx / 2) {
+        x += Lx; x0 += Lx;
+        if (MODE & NZ_MODE_PHI) kahan_add(fx, kx, Lx * Ga);
+      } else if (x > Lx / 2) {
+        x -= Lx; x0 -= Lx;
+        if (MODE & NZ_MODE_PHI) kahan_add(fx, kx, -(Lx * Ga));
+      }
+      if (y < -Ly / 2) {
+        y += Ly; y0 += Ly;
+        if (MODE & NZ_MODE_PHI) kahan_add(fy, ky, Ly * Ga);
+      } else if (y > Ly / 2) {
+        y -= Ly; y0 -= Ly;
+        if (MODE & NZ_MODE_PHI) kahan_add(fy, ky, -(Ly * Ga));
+      }
+      if (z < -Lz / 2) {
+        z += Lz; z0 += Lz;
+        if (MODE & NZ_MODE_PHI) kahan_add(fz, kz, Lz * Ga);
+      } else if (z > Lz / 2) {
+        z -= Lz; z0 -= Lz;
+        if (MODE & NZ_MODE_PHI) kahan_add(fz, kz, -(Lz * Ga));
+      }
+      if (MODE & NZ_MODE_MOMENTS) {
+        const float ex = x - x0, ey = y - y0, ez = z - z0;
+        float* m = s_mom + 6 * (s - s0);
+        const float ex2 = ex * ex, ey2 = ey * ey, ez2 = ez * ez;
+        atomicAdd(m + 0, ex2);
+        atomicAdd(m + 1, ey2);
+        atomicAdd(m + 2, ez2);
+        atomicAdd(m + 3, ex2 * ex2);
+        atomicAdd(m + 4, ey2 * ey2);
+        atomicAdd(m + 5, ez2 * ez2);
+      }
+      s++;
+      niter = 0;
+    }
+  }
+  J.pos[w] = make_float4(x, y, z, __int_as_float(label));
+  J.org[w] = make_float4(x0, y0, z0, O.w);
+  if (MODE & (NZ_MODE_PHI | NZ_MODE_SIG)) J.phi[w] = make_float4(fx, fy, fz, sig);
+  J.comp[w] = make_float4(kx, ky, kz, __int_as_float(flags));
+}
+
+// Work items are CTAs' worth of walkers of one job.  SINGLE: one job passed by
+// value, item i = walkers [i*T, i*T + T).  Otherwise jobs and items come from
+// device arrays; with queue != null the grid is persistent and each CTA takes
+// items from *queue until none is left.
+template <int MODE, bool SINGLE>
+__global__ void __launch_bounds__(kFusedThreads) walk_fused_kernel(const JobDev single, const nz_job* __restrict__ jobs,
+                                                                   const nz_item* __restrict__ items, int n_items,
+                                                                   int step0, int step1, int* queue) {
+  __shared__ int s_item;
+  __shared__ float s_mom[(MODE & NZ_MODE_MOMENTS) ? kMomentSteps * 6 : 1];
+  int it = blockIdx.x;
+  for (;;) {
+    if (queue) {
+      if (threadIdx.x == 0) s_item = atomicAdd(queue, 1);
+      __syncthreads();
+      it = s_item;
+      __syncthreads();
+    }
+    if (it >= n_items) return;
+    nz_item wi;
+    JobDev J;
+    if (SINGLE) {
+      J = single;
+      wi.job = 0;
+      wi.first = it * kFusedThreads;
+      wi.count = min(kFusedThreads, J.nwalkers - wi.first);
+    } else {
+      wi = items[it];
+      const nz_job& a = jobs[wi.job];
+      J = make_job(a.sub, a.G, a.Garea, a.nsteps, a.dt, a.draws, a.mode, a.state, a.moments);
+    }
+    const int s0 = step0, s1 = min(step1, J.nsteps);
+    if (MODE & NZ_MODE_MOMENTS) {
+      for (int i = threadIdx.x; i < kMomentSteps * 6; i += blockDim.x) s_mom[i] = 0.0f;
+      __syncthreads();
+    }
+    if (threadIdx.x < wi.count && s0 < s1) walk_one<MODE>(J, wi.first + threadIdx.x, s0, s1, s_mom);
+    if (MODE & NZ_MODE_MOMENTS) {
+      __syncthreads();
+      if (J.moments)
+        for (int i = threadIdx.x; i < (s1 - s0) * 6; i += blockDim.x)
+          atomicAdd(J.moments + size_t(s0) * 6 + i, double(s_mom[i]));
+      __syncthreads();
+    }
+    if (!queue) return;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// packing between the reference layout and the fused state
+// ---------------------------------------------------------------------------
+__global__ void pack_kernel(nz_walkers wk, const uint32_t* __restrict__ ids, nz_state st) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= wk.N) return;
+  const int N = wk.N;
+  const int label = wk.label ? wk.label[w] : -1;
+  reinterpret_cast<float4*>(st.pos)[w] =
+      make_float4(wk.spins[w], wk.spins[N + w], wk.spins[2 * N + w], __int_as_float(label));
+  reinterpret_cast<float4*>(st.org)[w] =
+      make_float4(wk.spins0[w], wk.spins0[N + w], wk.spins0[2 * N + w], __uint_as_float(ids ? ids[w] : uint32_t(w)));
+  float4 f = make_float4(0.f, 0.f, 0.f, wk.sig ? wk.sig[w] : 1.0f);
+  float4 c = make_float4(0.f, 0.f, 0.f, __int_as_float(wk.flags ? wk.flags[w] : 0));
+  if (wk.phi) {
+    f.x = wk.phi[w]; f.y = wk.phi[N + w]; f.z = wk.phi[2 * N + w];
+    c.x = wk.phi[3 * N + w]; c.y = wk.phi[4 * N + w]; c.z = wk.phi[5 * N + w];
+  }
+  reinterpret_cast<float4*>(st.phi)[w] = f;
+  reinterpret_cast<float4*>(st.comp)[w] = c;
+}
+
+__global__ void unpack_kernel(nz_state st, nz_walkers wk) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= wk.N) return;
+  const int N = wk.N;
+  const float4 p = reinterpret_cast<const float4*>(st.pos)[w];
+  const float4 o = reinterpret_cast<const float4*>(st.org)[w];
+  const float4 f = reinterpret_cast<const float4*>(st.phi)[w];
+  const float4 c = reinterpret_cast<const float4*>(st.comp)[w];
+  wk.spins[w] = p.x; wk.spins[N + w] = p.y; wk.spins[2 * N + w] = p.z;
+  wk.spins0[w] = o.x; wk.spins0[N + w] = o.y; wk.spins0[2 * N + w] = o.z;
+  if (wk.label) wk.label[w] = __float_as_int(p.w);
+  if (wk.sig) wk.sig[w] = f.w;
+  if (wk.flags) wk.flags[w] = __float_as_int(c.w);
+  if (wk.phi) {
+    wk.phi[w] = f.x; wk.phi[N + w] = f.y; wk.phi[2 * N + w] = f.z;
+    wk.phi[3 * N + w] = c.x; wk.phi[4 * N + w] = c.y; wk.phi[5 * N + w] = c.z;
+  }
+}
+
+__host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, const float* Garea, int nsteps, float dt,
+                                    const nz_draws& d, int mode, const nz_state& st, double* moments) {
+  JobDev j;
+  j.nwalkers = st.N;
+  j.g = Grid{sub.grid.Lx, sub.grid.Ly, sub.grid.Lz, sub.grid.dLx, sub.grid.dLy, sub.grid.dLz,
+             float(sub.grid.nx), float(sub.grid.ny), float(sub.grid.nz)};
+  j.nstructures = sub.nstructures;
+  j.sph4 = reinterpret_cast<const float4*>(sub.cell_sph4);
+  j.sid = sub.cell_sid;
+  j.cell_start = sub.cell_start;
+  j.cell_count = sub.cell_count;
+  j.D = sub.D;
+  j.T2 = sub.T2;
+  j.G = G;
+  j.Garea = Garea;
+  j.nsteps = nsteps;
+  j.dt = dt;
+  j.key0 = d.key0;
+  j.key1 = d.key1;
+  j.stream = d.stream;
+  j.mode = mode;
+  j.pos = reinterpret_cast<float4*>(st.pos);
+  j.org = reinterpret_cast<float4*>(st.org);
+  j.phi = reinterpret_cast<float4*>(st.phi);
+  j.comp = reinterpret_cast<float4*>(st.comp);
+  j.moments = moments;
+  return j;
+}
+
+template <int MODE>
+void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0, int step1,
+                 int* queue, int grid, cudaStream_t st) {
+  if (jobs)
+    walk_fused_kernel<MODE, false><<<grid, kFusedThreads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
+  else
+    walk_fused_kernel<MODE, true><<<grid, kFusedThreads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
+}
+
+// jobs == null: the single job `single` with n_items CTAs of kFusedThreads walkers.
+int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
+                 int step1, int* queue, int grid, cudaStream_t st) {
+  switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS)) {
+    case NZ_MODE_PHI: launch_mode<NZ_MODE_PHI>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+    case NZ_MODE_SIG: launch_mode<NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+    case NZ_MODE_PHI | NZ_MODE_SIG:
+      launch_mode<NZ_MODE_PHI | NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+    case NZ_MODE_SIG | NZ_MODE_MOMENTS:
+      launch_mode<NZ_MODE_SIG | NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+    case NZ_MODE_MOMENTS:
+      launch_mode<NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+    case 0: launch_mode<0>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+    default: return set_error(NZ_ERR_ARG, "fused walk: unsupported mode %d", mode);
+  }
+  return check_launch("walk_fused_kernel");
+}
+
+}  // namespace nz

@@ -1,0 +1,255 @@
+// Seeding, walker re-binning, signal and moment reductions.
+#include <cstdint>
+#include "kernels.cuh"
+
+namespace nz {
+
+// ---------------------------------------------------------------------------
+// Seeding: seedSpinsKernel's acceptance rule (sim3d_kernel.cu:240-337) with
+// the rounds of SimGeometry3D.gpu_seed (geometry.py:146-168) moved inside the
+// kernel and bounded.  The label of a point is found from its cell's list:
+// every sphere that contains a point of a cell is a member of that cell.
+// ---------------------------------------------------------------------------
+__global__ void seed_kernel(nz_substrate sub, const uint8_t* __restrict__ target, int N, uint32_t k0, uint32_t k1,
+                            uint32_t stream, int max_rounds, float* __restrict__ spins, int* __restrict__ label,
+                            int* __restrict__ n_unseeded) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= N) return;
+  const Grid g{sub.grid.Lx, sub.grid.Ly, sub.grid.Lz, sub.grid.dLx, sub.grid.dLy, sub.grid.dLz,
+               float(sub.grid.nx), float(sub.grid.ny), float(sub.grid.nz)};
+  const int S = sub.S;
+  const float* __restrict__ cx = sub.spheres;
+  const float* __restrict__ rr = sub.spheres + 3 * S;
+  const float* __restrict__ sphSID = sub.spheres + 4 * S;
+  const int ns = sub.nstructures;
+  for (int round = 0; round < max_rounds; ++round) {
+    float u0, u1, u2;
+    philox_uniform3(k0, k1, stream, uint32_t(w), uint32_t(round), u0, u1, u2);
+    const float px = (u0 - 0.5f) * g.Lx;
+    const float py = (u1 - 0.5f) * g.Ly;
+    const float pz = (u2 - 0.5f) * g.Lz;
+    const int cell = cell_of(g, px, py, pz);
+    const int start = sub.cell_start[cell], count = sub.cell_count[cell];
+    int lab = ns;
+    for (int n = 0; n < count; ++n) {
+      const int s = sub.cell_items[start + n];
+      const float dx = px - cx[s], dy = py - cx[S + s], dz = pz - cx[2 * S + s];
+      const int sid = int(sphSID[s]);
+      if (dx * dx + dy * dy + dz * dz < rr[s] * rr[s] && sid < lab) lab = sid;
+    }
+    bool accept;
+    if (lab < ns) accept = target[lab] != 0;
+    else accept = target[ns] != 0 && px > -g.Lx / 2 && px < g.Lx / 2 && py > -g.Ly / 2 && py < g.Ly / 2 &&
+                  pz > -g.Lz / 2 && pz < g.Lz / 2;
+    if (accept) {
+      spins[w] = px;
+      spins[N + w] = py;
+      spins[2 * N + w] = pz;
+      if (label) label[w] = lab;
+      return;
+    }
+  }
+  if (label) label[w] = -1;
+  atomicAdd(n_unseeded, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Re-binning: counting sort of the packed walker state by coarse cell.
+// ---------------------------------------------------------------------------
+struct BinGrid {
+  Grid g;
+  int cx, cy, cz;     // coarsening per axis
+  int bx, by, bz;     // bins per axis
+};
+
+__device__ __forceinline__ int bin_of(const BinGrid& b, float x, float y, float z) {
+  const int c = cell_of(b.g, x, y, z);
+  const int nx = int(b.g.nLx), ny = int(b.g.nLy);
+  const int ix = c % nx, iy = (c / nx) % ny, iz = c / (nx * ny);
+  return ((iz / b.cz) * b.by + iy / b.cy) * b.bx + ix / b.cx;
+}
+
+__global__ void bin_count_kernel(const float4* __restrict__ pos, int N, BinGrid b, int* __restrict__ bins,
+                                 int* __restrict__ hist) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= N) return;
+  const float4 p = pos[w];
+  const int k = bin_of(b, p.x, p.y, p.z);
+  bins[w] = k;
+  atomicAdd(hist + k, 1);
+}
+
+__global__ void bin_scatter_kernel(nz_state in, int N, const int* __restrict__ bins, int* __restrict__ cursor,
+                                   nz_state out) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= N) return;
+  const int slot = atomicAdd(cursor + bins[w], 1);
+  reinterpret_cast<float4*>(out.pos)[slot] = reinterpret_cast<const float4*>(in.pos)[w];
+  reinterpret_cast<float4*>(out.org)[slot] = reinterpret_cast<const float4*>(in.org)[w];
+  reinterpret_cast<float4*>(out.phi)[slot] = reinterpret_cast<const float4*>(in.phi)[w];
+  reinterpret_cast<float4*>(out.comp)[slot] = reinterpret_cast<const float4*>(in.comp)[w];
+}
+
+// ---------------------------------------------------------------------------
+// Signal: S[d][b] += sum_w exp(i amp[b] u_d . Phi_w); FP32 per walker, FP64
+// block sums, one FP64 atomic per block and (d, b).
+// ---------------------------------------------------------------------------
+constexpr int kSigThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* s_red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? s_red[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  return t;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(kSigThreads) signal_kernel(nz_state st, const float* __restrict__ dirs, int ndir,
+                                                             const float* __restrict__ amp, int nb,
+                                                             double* __restrict__ out) {
+  __shared__ double s_red[32];
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  float px = 0.f, py = 0.f, pz = 0.f;
+  const bool live = w < st.N;
+  if (live) {
+    const float4 f = reinterpret_cast<const float4*>(st.phi)[w];
+    const float4 c = reinterpret_cast<const float4*>(st.comp)[w];
+    px = f.x - c.x;
+    py = f.y - c.y;
+    pz = f.z - c.z;
+  }
+  for (int d = 0; d < ndir; ++d) {
+    const float ph = px * __ldg(dirs + d) + py * __ldg(dirs + ndir + d) + pz * __ldg(dirs + 2 * ndir + d);
+    for (int b = 0; b < nb; ++b) {
+      float sn = 0.f, cs = 0.f;
+      if (live) sincosf(__ldg(amp + b) * ph, &sn, &cs);
+      const double re = block_sum(live ? double(cs) : 0.0, s_red);
+      const double im = block_sum(live ? double(sn) : 0.0, s_red);
+      if (threadIdx.x == 0) {
+        atomicAdd(out + d * nb + b, re);
+        atomicAdd(out + ndir * nb + d * nb + b, im);
+      }
+    }
+  }
+}
+
+__global__ void phase_from_phi_kernel(nz_state st, const float* __restrict__ dirs, int ndir, float* __restrict__ phase) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= st.N) return;
+  const float4 f = reinterpret_cast<const float4*>(st.phi)[w];
+  const float4 c = reinterpret_cast<const float4*>(st.comp)[w];
+  const float px = f.x - c.x, py = f.y - c.y, pz = f.z - c.z;
+  for (int d = 0; d < ndir; ++d)
+    phase[size_t(d) * st.N + w] = px * dirs[d] + py * dirs[ndir + d] + pz * dirs[2 * ndir + d];
+}
+
+// computeDiffusionCoefficientsAndKurtosis's sums (sim3d_kernel.cu:193-200) in FP64.
+__global__ void __launch_bounds__(256) moments_kernel(const float* __restrict__ spins, const float* __restrict__ spins0,
+                                                      int N, double* __restrict__ out) {
+  __shared__ double s_red[32];
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  double m[6] = {0, 0, 0, 0, 0, 0};
+  if (w < N) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float d = spins[size_t(a) * N + w] - spins0[size_t(a) * N + w];
+      const double d2 = double(d) * double(d);
+      m[a] = d2;
+      m[3 + a] = d2 * d2;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const double t = block_sum(m[i], s_red);
+    if (threadIdx.x == 0) atomicAdd(out + i, t);
+  }
+}
+
+}  // namespace nz
+
+using namespace nz;
+
+extern "C" int nz_seed(const nz_substrate* sub, const uint8_t* target, int N, uint32_t key0, uint32_t key1,
+                       uint32_t stream_id, int max_rounds, float* spins, int* label, int* n_unseeded, void* stream) {
+  if (!sub || !target || N < 0 || max_rounds <= 0 || !spins || !n_unseeded || !sub->cell_start || !sub->cell_count ||
+      !sub->cell_items || (sub->S > 0 && !sub->spheres))
+    return set_error(NZ_ERR_ARG, "nz_seed: bad arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(n_unseeded, 0, sizeof(int), st) != cudaSuccess) return check_launch("nz_seed memset");
+  if (N == 0) return NZ_OK;
+  seed_kernel<<<(N + 255) / 256, 256, 0, st>>>(*sub, target, N, key0, key1, stream_id, max_rounds, spins, label,
+                                                n_unseeded);
+  return check_launch("seed_kernel");
+}
+
+static inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+extern "C" size_t nz_sort_scratch_bytes(int N, int nbins) {
+  if (N < 0 || nbins < 0) return 0;
+  return align256(size_t(N) * sizeof(int)) + 2 * align256(size_t(nbins) * sizeof(int));
+}
+
+extern "C" int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out, void* scratch,
+                             size_t scratch_bytes, void* stream) {
+  if (!in || !grid || !out || coarsen <= 0 || in->N != out->N || !scratch)
+    return set_error(NZ_ERR_ARG, "nz_state_sort: bad arguments");
+  BinGrid b;
+  b.g = Grid{grid->Lx, grid->Ly, grid->Lz, grid->dLx, grid->dLy, grid->dLz, float(grid->nx), float(grid->ny),
+             float(grid->nz)};
+  b.cx = b.cy = b.cz = coarsen;
+  b.bx = (grid->nx + coarsen - 1) / coarsen;
+  b.by = (grid->ny + coarsen - 1) / coarsen;
+  b.bz = (grid->nz + coarsen - 1) / coarsen;
+  const long long nbins = 1ll * b.bx * b.by * b.bz;
+  if (nbins > (1 << 26)) return set_error(NZ_ERR_ARG, "nz_state_sort: %lld bins, coarsen more", nbins);
+  const int N = in->N;
+  const size_t need = nz_sort_scratch_bytes(N, int(nbins));
+  if (scratch_bytes < need)
+    return set_error(NZ_ERR_CAPACITY, "nz_state_sort: scratch %zu bytes < %zu", scratch_bytes, need);
+  if (N == 0) return NZ_OK;
+  char* p = static_cast<char*>(scratch);
+  int* bins = reinterpret_cast<int*>(p);
+  int* hist = reinterpret_cast<int*>(p + align256(size_t(N) * sizeof(int)));
+  int* cursor = reinterpret_cast<int*>(p + align256(size_t(N) * sizeof(int)) + align256(size_t(nbins) * sizeof(int)));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(hist, 0, size_t(nbins) * sizeof(int), st) != cudaSuccess) return check_launch("sort memset");
+  bin_count_kernel<<<(N + 255) / 256, 256, 0, st>>>(reinterpret_cast<const float4*>(in->pos), N, b, bins, hist);
+  int rc = check_launch("bin_count_kernel");
+  if (rc) return rc;
+  scan_kernel<<<1, 1024, 0, st>>>(hist, cursor, int(nbins), nullptr);
+  rc = check_launch("scan_kernel");
+  if (rc) return rc;
+  bin_scatter_kernel<<<(N + 255) / 256, 256, 0, st>>>(*in, N, bins, cursor, *out);
+  return check_launch("bin_scatter_kernel");
+}
+
+extern "C" int nz_signal_phi(const nz_state* st, const float* dirs, int ndir, const float* amp, int nb, double* out,
+                             void* stream) {
+  if (!st || !dirs || !amp || !out || ndir <= 0 || nb <= 0) return set_error(NZ_ERR_ARG, "nz_signal_phi: bad arguments");
+  if (st->N == 0) return NZ_OK;
+  signal_kernel<<<(st->N + kSigThreads - 1) / kSigThreads, kSigThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      *st, dirs, ndir, amp, nb, out);
+  return check_launch("signal_kernel");
+}
+
+extern "C" int nz_phase_from_phi(const nz_state* st, const float* dirs, int ndir, float* phase, void* stream) {
+  if (!st || !dirs || !phase || ndir <= 0) return set_error(NZ_ERR_ARG, "nz_phase_from_phi: bad arguments");
+  if (st->N == 0) return NZ_OK;
+  phase_from_phi_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*st, dirs, ndir, phase);
+  return check_launch("phase_from_phi_kernel");
+}
+
+extern "C" int nz_moments(const float* spins, const float* spins0, int N, double* out, void* stream) {
+  if (!spins || !spins0 || !out || N < 0) return set_error(NZ_ERR_ARG, "nz_moments: bad arguments");
+  if (N == 0) return NZ_OK;
+  moments_kernel<<<(N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(spins, spins0, N, out);
+  return check_launch("moments_kernel");
+}

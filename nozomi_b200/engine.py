@@ -1,0 +1,284 @@
+"""Device-side objects over the C ABI: substrates with their cell lists, walker
+state, and the walk / seeding / reduction calls.
+
+PyTorch provides device memory and the current stream; every computation is a
+kernel of libnozomi_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from ._lib import NozomiError
+
+
+def require_cuda():
+    if not torch.cuda.is_available():
+        raise NozomiError("nozomi_b200 needs a CUDA device (sm_100a); there is no CPU path")
+    L.load()
+
+
+def _p(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev():
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def box_grid(L3, nseg) -> L.Grid:
+    """The reference's float constants Lx.. and dLx = Lx / nseg (diffsim3d.py:115-120)."""
+    Lx, Ly, Lz = (float(v) for v in L3)
+    nx, ny, nz = (int(v) for v in nseg)
+    return L.Grid(np.float32(Lx), np.float32(Ly), np.float32(Lz), np.float32(Lx / nx), np.float32(Ly / ny),
+                  np.float32(Lz / nz), nx, ny, nz)
+
+
+class DeviceSubstrate:
+    """Spheres [5,S] (cx, cy, cz, r, structure id), box, cell grid, compact cell
+    lists built on the GPU (DiffSim3d.set_segments, diffsim3d.py:107-174), the
+    per-entry sphere records of the fused walk, and D / T2 per structure."""
+
+    def __init__(self, spheres: np.ndarray, nstructures: int, L3, nseg, D, T2, jump_tol: float = 1.0,
+                 cells: tuple | None = None):
+        require_cuda()
+        dev = _dev()
+        sph64 = np.ascontiguousarray(spheres, dtype=np.float64).reshape(5, -1)
+        self.S = sph64.shape[1]
+        self.nstructures = int(nstructures)
+        self.L = tuple(float(v) for v in L3)
+        self.nseg = tuple(int(v) for v in nseg)
+        self.ncell = self.nseg[0] * self.nseg[1] * self.nseg[2]
+        self.jump_tol = float(jump_tol)
+        self.grid = box_grid(self.L, self.nseg)
+        self.spheres64 = torch.from_numpy(sph64).to(dev)
+        self.spheres = torch.from_numpy(sph64.astype(np.float32)).to(dev)
+        self.D = torch.as_tensor(np.asarray(D, np.float32), device=dev)
+        self.T2 = torch.as_tensor(np.asarray(T2, np.float32), device=dev)
+        if self.D.numel() != self.nstructures + 1 or self.T2.numel() != self.nstructures + 1:
+            raise NozomiError("D and T2 need one entry per structure plus the box")
+        if cells is None:
+            self._build_cells()
+        else:
+            st, ct, it = cells
+            self.cell_start = torch.as_tensor(np.asarray(st, np.int32), device=dev)
+            self.cell_count = torch.as_tensor(np.asarray(ct, np.int32), device=dev)
+            self.cell_items = torch.as_tensor(np.asarray(it, np.int32), device=dev)
+        self._gather()
+
+    def _build_cells(self):
+        dev = _dev()
+        lib = L.load()
+        Lx, Ly, Lz = self.L
+        nx, ny, nz = self.nseg
+        counts = torch.empty(self.ncell, dtype=torch.int32, device=dev)
+        L.check(lib.nz_cells_count(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, self.jump_tol, _p(counts),
+                                   _stream()), "nz_cells_count")
+        offsets = torch.empty(self.ncell, dtype=torch.int32, device=dev)
+        total = torch.zeros(1, dtype=torch.int32, device=dev)
+        L.check(lib.nz_exclusive_scan_i32(_p(counts), _p(offsets), self.ncell, _p(total), _stream()),
+                "nz_exclusive_scan_i32")
+        n_items = int(total.item())  # one host sync: the list length sizes the item array
+        items = torch.empty(max(n_items, 1), dtype=torch.int32, device=dev)
+        cursor = torch.empty(self.ncell, dtype=torch.int32, device=dev)
+        L.check(lib.nz_cells_fill(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, self.jump_tol, _p(offsets),
+                                  _p(counts), _p(cursor), _p(items), _stream()), "nz_cells_fill")
+        self.cell_start, self.cell_count, self.cell_items = offsets, counts, items
+        self.n_items = n_items
+
+    def _gather(self):
+        dev = _dev()
+        n = int(self.cell_items.numel())
+        self.n_items = n
+        self.cell_sph4 = torch.empty((max(n, 1), 4), dtype=torch.float32, device=dev)
+        self.cell_sid = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+        L.check(L.load().nz_cells_gather(_p(self.spheres), self.S, _p(self.cell_items), n, _p(self.cell_sph4),
+                                         _p(self.cell_sid), _stream()), "nz_cells_gather")
+
+    def max_count(self) -> int:
+        return int(self.cell_count.max().item()) if self.ncell else 0
+
+    def padded_segments(self, K: int | None = None) -> tuple[int, torch.Tensor]:
+        """The reference's padded table (K, segments[ncell*K])."""
+        K = self.max_count() if K is None else int(K)
+        seg = torch.empty(self.ncell * K, dtype=torch.int32, device=_dev())
+        Lx, Ly, Lz = self.L
+        nx, ny, nz = self.nseg
+        L.check(L.load().nz_segments_fill(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, K, _p(seg), _stream()),
+                "nz_segments_fill")
+        return K, seg
+
+    def with_padded_lists(self) -> "DeviceSubstrate":
+        """A view whose cell lists are the reference's padded table."""
+        K, seg = self.padded_segments()
+        other = object.__new__(DeviceSubstrate)
+        other.__dict__.update(self.__dict__)
+        dev = _dev()
+        other.cell_start = torch.arange(self.ncell, dtype=torch.int32, device=dev) * K
+        other.cell_count = torch.full((self.ncell,), K, dtype=torch.int32, device=dev)
+        other.cell_items = seg
+        other._gather()
+        other.K = K
+        return other
+
+    def struct(self) -> L.Substrate:
+        return L.Substrate(self.grid, self.nstructures, self.S, self.spheres.data_ptr(), self.cell_start.data_ptr(),
+                           self.cell_count.data_ptr(), self.cell_items.data_ptr(), self.cell_sph4.data_ptr(),
+                           self.cell_sid.data_ptr(), self.D.data_ptr(), self.T2.data_ptr())
+
+    def nbytes(self) -> int:
+        ts = [self.spheres64, self.spheres, self.D, self.T2, self.cell_start, self.cell_count, self.cell_items,
+              self.cell_sph4, self.cell_sid]
+        return sum(t.numel() * t.element_size() for t in ts)
+
+
+def philox_draws(key: int, stream_id: int = 0) -> L.Draws:
+    key = int(key) & 0xFFFFFFFFFFFFFFFF
+    return L.Draws(None, 0, 0, key & 0xFFFFFFFF, (key >> 32) & 0xFFFFFFFF, stream_id & 0xFFFFFFFF)
+
+
+def injected_draws(table: torch.Tensor) -> L.Draws:
+    """table: [N, nsteps, maxk] float32 on the device."""
+    return L.Draws(table.data_ptr(), int(table.shape[1]), int(table.shape[2]), 0, 0, 0)
+
+
+def seed(sub: DeviceSubstrate, targets, N: int, key: int, max_rounds: int = 100000, stream_id: int = 1):
+    """Seed N walkers uniformly into the target structures (the box is
+    structure sub.nstructures).  Returns (spins [3,N] float32, label [N])."""
+    dev = _dev()
+    tgt = np.zeros(sub.nstructures + 1, np.uint8)
+    tgt[np.asarray(list(targets), np.int64)] = 1
+    tgt_d = torch.from_numpy(tgt).to(dev)
+    spins = torch.empty((3, N), dtype=torch.float32, device=dev)
+    label = torch.empty(N, dtype=torch.int32, device=dev)
+    left = torch.zeros(1, dtype=torch.int32, device=dev)
+    s = sub.struct()
+    key = int(key) & 0xFFFFFFFFFFFFFFFF
+    L.check(L.load().nz_seed(L.byref(s), _p(tgt_d), N, key & 0xFFFFFFFF, key >> 32, stream_id, max_rounds, _p(spins),
+                             _p(label), _p(left), _stream()), "nz_seed")
+    n_left = int(left.item())
+    if n_left:
+        raise NozomiError(f"seeding left {n_left} of {N} walkers unplaced after {max_rounds} rounds "
+                          f"(target structures {sorted(set(int(t) for t in targets))} may have no volume)")
+    return spins, label
+
+
+@dataclass
+class Walkers:
+    """Walker arrays in the reference's layout (diffsim3d.py:42-45, :62)."""
+    spins: torch.Tensor               # [3, N]
+    spins0: torch.Tensor              # [3, N]
+    phase: torch.Tensor | None = None     # [ndir, N]
+    diffdir: torch.Tensor | None = None   # [3, ndir]
+    sig: torch.Tensor | None = None       # [N]
+    phi: torch.Tensor | None = None       # [6, N]
+    label: torch.Tensor | None = None
+    n_iter: torch.Tensor | None = None
+    n_scatter: torch.Tensor | None = None
+    flags: torch.Tensor | None = None
+
+    @property
+    def N(self) -> int:
+        return int(self.spins.shape[1])
+
+    def struct(self) -> L.Walkers:
+        nd = 0 if self.diffdir is None else int(self.diffdir.shape[1])
+        v = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        return L.Walkers(self.N, v(self.spins), v(self.spins0), v(self.phase), v(self.diffdir), nd, v(self.sig),
+                         v(self.phi), v(self.label), v(self.n_iter), v(self.n_scatter), v(self.flags))
+
+    @staticmethod
+    def with_counters(spins, spins0, **kw) -> "Walkers":
+        N = spins.shape[1]
+        dev = spins.device
+        z = lambda: torch.zeros(N, dtype=torch.int32, device=dev)  # noqa: E731
+        return Walkers(spins, spins0, label=z(), n_iter=z(), n_scatter=z(), flags=z(), **kw)
+
+
+def walk_step(sub: DeviceSubstrate, wk: Walkers, mode: int, dt: float, G: float, Garea: float, step: int,
+              draws: L.Draws):
+    s = sub.struct()
+    w = wk.struct()
+    L.check(L.load().nz_walk_step(L.byref(s), L.byref(w), mode, np.float32(dt), np.float32(G), np.float32(Garea),
+                                  int(step), L.byref(draws), _stream()), "nz_walk_step")
+
+
+class FusedState:
+    """Packed walkers of the fused walk: four float4 per walker."""
+
+    def __init__(self, N: int):
+        dev = _dev()
+        self.N = N
+        self.pos = torch.empty((N, 4), dtype=torch.float32, device=dev)
+        self.org = torch.empty((N, 4), dtype=torch.float32, device=dev)
+        self.phi = torch.empty((N, 4), dtype=torch.float32, device=dev)
+        self.comp = torch.empty((N, 4), dtype=torch.float32, device=dev)
+
+    def struct(self) -> L.State:
+        return L.State(self.N, self.pos.data_ptr(), self.org.data_ptr(), self.phi.data_ptr(), self.comp.data_ptr())
+
+    def nbytes(self) -> int:
+        return 4 * 16 * self.N
+
+    @staticmethod
+    def from_walkers(wk: Walkers, ids: torch.Tensor | None = None) -> "FusedState":
+        st = FusedState(wk.N)
+        s = st.struct()
+        w = wk.struct()
+        L.check(L.load().nz_state_pack(L.byref(w), _p(ids), L.byref(s), _stream()), "nz_state_pack")
+        return st
+
+    def to_walkers(self, wk: Walkers):
+        s = self.struct()
+        w = wk.struct()
+        L.check(L.load().nz_state_unpack(L.byref(s), L.byref(w), _stream()), "nz_state_unpack")
+
+    def walker_ids(self) -> torch.Tensor:
+        return self.org[:, 3].contiguous().view(torch.int32)
+
+    def sort_into(self, other: "FusedState", grid: L.Grid, coarsen: int, scratch: torch.Tensor | None = None):
+        nb = (-(-grid.nx // coarsen)) * (-(-grid.ny // coarsen)) * (-(-grid.nz // coarsen))
+        need = int(L.load().nz_sort_scratch_bytes(self.N, nb))
+        if scratch is None or scratch.numel() < need:
+            scratch = torch.empty(need, dtype=torch.uint8, device=_dev())
+        a, b = self.struct(), other.struct()
+        L.check(L.load().nz_state_sort(L.byref(a), L.byref(grid), coarsen, L.byref(b), _p(scratch), scratch.numel(),
+                                       _stream()), "nz_state_sort")
+        return scratch
+
+    def signal(self, dirs: torch.Tensor, amps: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Sum over walkers of exp(i amp_b u_d . Phi): [2, ndir, nb] float64."""
+        ndir, nb = int(dirs.shape[1]), int(amps.numel())
+        if out is None:
+            out = torch.zeros((2, ndir, nb), dtype=torch.float64, device=_dev())
+        s = self.struct()
+        L.check(L.load().nz_signal_phi(L.byref(s), _p(dirs), ndir, _p(amps), nb, _p(out), _stream()), "nz_signal_phi")
+        return out
+
+    def phase(self, dirs: torch.Tensor) -> torch.Tensor:
+        ndir = int(dirs.shape[1])
+        out = torch.empty((ndir, self.N), dtype=torch.float32, device=_dev())
+        s = self.struct()
+        L.check(L.load().nz_phase_from_phi(L.byref(s), _p(dirs), ndir, _p(out), _stream()), "nz_phase_from_phi")
+        return out
+
+
+def walk_fused(sub: DeviceSubstrate, st: FusedState, mode: int, dt: float, G: torch.Tensor | None,
+               Garea: torch.Tensor | None, step0: int, step1: int, draws: L.Draws,
+               moments: torch.Tensor | None = None):
+    s = sub.struct()
+    a = st.struct()
+    L.check(L.load().nz_walk_fused(L.byref(s), L.byref(a), mode, np.float32(dt), _p(G), _p(Garea), int(step0),
+                                   int(step1), L.byref(draws), _p(moments), _stream()), "nz_walk_fused")
+
+
+def moments(spins: torch.Tensor, spins0: torch.Tensor, out: torch.Tensor):
+    L.check(L.load().nz_moments(_p(spins), _p(spins0), int(spins.shape[1]), _p(out), _stream()), "nz_moments")

@@ -298,7 +298,8 @@ OZ_API void oz_moments(int N, const float* spins, const float* spins0, double* o
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int w = 0; w < N; ++w)
         for (int a = 0; a < 3; ++a) {
-            double d = (double)spins[a*N + w] - (double)spins0[a*N + w];
+            /* the displacement in float, as sim3d_kernel.cu:193-195 forms it */
+            double d = (double)(spins[a*N + w] - spins0[a*N + w]);
             acc[a] += d*d;
             acc[3 + a] += d*d*d*d;
         }

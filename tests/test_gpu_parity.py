@@ -1,0 +1,256 @@
+"""GPU parity: the CUDA kernels against the oracle and the reference's own
+outputs (golden fixtures), through the C ABI.
+
+Bar: bit-exact for cell lists, labels, collision counts, positions, spins0,
+phase and Phi (same draws, same cell lists); T2 signal within 2e-6 relative
+(expf ulps); FP64 signal sums within 1e-9 absolute of the oracle's (FP32 sincos
+per walker, different summation order).
+"""
+import numpy as np
+import pytest
+
+from tests._fixtures import DWI, NARROW, dirs_of, load, oracle_geometry
+from oracle import oracle as oz
+from oracle.cells_oracle import cells_members, segments_reference
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    from nozomi_b200 import engine
+    engine.require_cuda()
+    return engine
+
+
+def _dev(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.cuda()
+
+
+def _sub_from_case(eng, c, padded=True):
+    nseg = tuple(int(v) for v in c["nseg"])
+    if padded:
+        from oracle.cells_oracle import padded_as_lists
+        ncell = nseg[0] * nseg[1] * nseg[2]
+        cells = padded_as_lists(int(c["K"]), c["segments"], ncell)
+    else:
+        cells = None
+    return eng.DeviceSubstrate(c["spheres"], int(c["nstructures"]), tuple(c["L"]), nseg, c["D"], c["T2"], cells=cells)
+
+
+def test_cells_match_oracle(eng):
+    z = np.load(__import__("tests._fixtures", fromlist=["GOLDEN"]).GOLDEN / "segments.npz")
+    for i in range(int(z["ncase"])):
+        sph, L3, nseg = z[f"case{i}_spheres"], tuple(z[f"case{i}_L"]), tuple(int(v) for v in z[f"case{i}_nseg"])
+        sub = eng.DeviceSubstrate(sph, 3, L3, nseg, np.full(4, 2.0), np.full(4, 100.0))
+        st, ct, it = cells_members(sph, L3, nseg)
+        np.testing.assert_array_equal(sub.cell_count.cpu().numpy(), ct)
+        np.testing.assert_array_equal(sub.cell_start.cpu().numpy(), st)
+        np.testing.assert_array_equal(sub.cell_items.cpu().numpy()[:it.size], it)
+        K, seg = sub.padded_segments()
+        K_ref, seg_ref = segments_reference(sph, L3, nseg)
+        assert K == K_ref == int(z[f"case{i}_K"])
+        np.testing.assert_array_equal(seg.cpu().numpy(), seg_ref)
+
+
+@pytest.mark.parametrize("name", NARROW)
+def test_plain_narrow_matches_reference(eng, name):
+    c = load(name)
+    sub = _sub_from_case(eng, c)
+    N = int(c["N"])
+    x = _dev(c["x0"])
+    wk = eng.Walkers.with_counters(x, x.clone(), sig=torch.ones(N, device="cuda"))
+    d = eng.philox_draws(int(c["key"]))
+    for s in range(int(c["nt"])):
+        eng.walk_step(sub, wk, eng.L.MODE_SIG, float(c["dt"]), 0.0, 0.0, s, d)
+    np.testing.assert_array_equal(wk.spins.cpu().numpy(), c["spins"])
+    np.testing.assert_array_equal(wk.spins0.cpu().numpy(), c["spins0"])
+    np.testing.assert_allclose(wk.sig.cpu().numpy(), c["sig"], rtol=2e-6)
+    # labels and collision counts against the oracle on the same inputs
+    g = oracle_geometry(c)
+    spins, spins0 = c["x0"].copy(), c["x0"].copy()
+    sig = np.ones(N, np.float32)
+    r = oz.walk_f32(g, oz.philox(int(c["key"])), oz.MODE_SIG, spins, spins0, 0, int(c["nt"]), float(c["dt"]), sig=sig)
+    np.testing.assert_array_equal(wk.label.cpu().numpy(), r["label"])
+    np.testing.assert_array_equal(wk.n_scatter.cpu().numpy(), r["n_scatter"])
+    np.testing.assert_array_equal(wk.n_iter.cpu().numpy(), r["n_iter"])
+    np.testing.assert_array_equal(wk.flags.cpu().numpy(), r["flags"])
+
+
+@pytest.mark.parametrize("name", DWI)
+def test_plain_dwi_matches_reference(eng, name):
+    c = load(name)
+    sub = _sub_from_case(eng, c)
+    N = int(c["N"])
+    dirs = dirs_of(c)
+    x = _dev(c["x0"].astype(np.float32))
+    wk = eng.Walkers.with_counters(x, x.clone(), phase=torch.zeros((dirs.shape[1], N), device="cuda"),
+                                   diffdir=_dev(dirs))
+    d = eng.philox_draws(int(c["key"]))
+    G, Ga = c["G"], c["Garea"]
+    for s in range(int(c["nt"])):
+        eng.walk_step(sub, wk, eng.L.MODE_PHASE, float(c["dt"]), float(G[s]), float(Ga[s]), s, d)
+    np.testing.assert_array_equal(wk.spins.cpu().numpy(), c["spins"])
+    np.testing.assert_array_equal(wk.spins0.cpu().numpy(), c["spins0"])
+    np.testing.assert_array_equal(wk.phase.cpu().numpy(), c["phase"])
+
+
+@pytest.mark.parametrize("name", DWI + NARROW[:2])
+def test_fused_matches_oracle_and_reference(eng, name):
+    """The fused kernel (one launch for all steps, Phi form) against the oracle
+    with the same cell lists: positions, spins0, labels and Phi bit-exact; and
+    positions against the reference's own outputs."""
+    c = load(name)
+    sub = _sub_from_case(eng, c)
+    N = int(c["N"])
+    nt = int(c["nt"])
+    dt = float(c["dt"])
+    G = c["G"] if "G" in c else np.zeros(nt, np.float32)
+    Ga = c["Garea"] if "Garea" in c else np.zeros(nt, np.float32)
+    x = _dev(c["x0"].astype(np.float32))
+    wk = eng.Walkers(x, x.clone(), phi=torch.zeros((6, N), device="cuda"),
+                     label=torch.full((N,), -1, dtype=torch.int32, device="cuda"),
+                     flags=torch.zeros(N, dtype=torch.int32, device="cuda"), sig=torch.ones(N, device="cuda"))
+    st = eng.FusedState.from_walkers(wk)
+    mode = eng.L.MODE_PHI | eng.L.MODE_SIG
+    eng.walk_fused(sub, st, mode, dt, _dev(G.astype(np.float32)), _dev(Ga.astype(np.float32)), 0, nt,
+                   eng.philox_draws(int(c["key"])))
+    st.to_walkers(wk)
+    g = oracle_geometry(c)
+    spins, spins0 = c["x0"].astype(np.float32).copy(), c["x0"].astype(np.float32).copy()
+    phi = np.zeros((6, N), np.float32)
+    sig = np.ones(N, np.float32)
+    r = oz.walk_f32(g, oz.philox(int(c["key"])), oz.MODE_PHI | oz.MODE_SIG, spins, spins0, 0, nt, dt, G=G,
+                    Garea=Ga, phi=phi, sig=sig)
+    np.testing.assert_array_equal(wk.spins.cpu().numpy(), spins)
+    np.testing.assert_array_equal(wk.spins.cpu().numpy(), c["spins"])
+    np.testing.assert_array_equal(wk.spins0.cpu().numpy(), spins0)
+    np.testing.assert_array_equal(wk.phi.cpu().numpy(), phi)
+    np.testing.assert_array_equal(wk.label.cpu().numpy(), r["label"])
+    np.testing.assert_array_equal(wk.flags.cpu().numpy(), r["flags"])
+    np.testing.assert_allclose(wk.sig.cpu().numpy(), sig, rtol=2e-6)
+
+
+def test_fused_chunked_and_sorted_equals_single_launch(eng):
+    """Splitting the steps over launches and re-binning walkers between them
+    changes nothing: draws are keyed by walker id and step."""
+    c = load("dwi_c1_cells")
+    sub = _sub_from_case(eng, c, padded=False)
+    N, nt, dt = int(c["N"]), int(c["nt"]), float(c["dt"])
+    G, Ga = _dev(c["G"]), _dev(c["Garea"])
+    x = _dev(c["x0"].astype(np.float32))
+
+    def fresh():
+        wk = eng.Walkers(x.clone(), x.clone(), phi=torch.zeros((6, N), device="cuda"))
+        return eng.FusedState.from_walkers(wk)
+
+    d = eng.philox_draws(99)
+    a = fresh()
+    eng.walk_fused(sub, a, eng.L.MODE_PHI, dt, G, Ga, 0, nt, d)
+    b = fresh()
+    tmp = eng.FusedState(N)
+    scratch = None
+    for s0 in range(0, nt, 700):
+        scratch = b.sort_into(tmp, sub.grid, 2, scratch)
+        b, tmp = tmp, b
+        eng.walk_fused(sub, b, eng.L.MODE_PHI, dt, G, Ga, s0, min(nt, s0 + 700), d)
+    ia = a.walker_ids().cpu().numpy()
+    ib = b.walker_ids().cpu().numpy()
+    oa, ob = np.argsort(ia), np.argsort(ib)
+    for t in ("pos", "org", "phi", "comp"):
+        np.testing.assert_array_equal(getattr(a, t).cpu().numpy()[oa], getattr(b, t).cpu().numpy()[ob])
+
+
+def test_compact_lists_match_oracle(eng):
+    """Compact (member-only) cell lists: GPU plain and fused kernels against the
+    oracle using the same compact lists."""
+    c = load("dwi_overlap")
+    sph, L3, nseg = c["spheres"], tuple(c["L"]), tuple(int(v) for v in c["nseg"])
+    sub = eng.DeviceSubstrate(sph, int(c["nstructures"]), L3, nseg, c["D"], c["T2"])
+    st_, ct, it = cells_members(sph, L3, nseg)
+    g = oz.Geometry(sph.astype(np.float32), int(c["nstructures"]), L3, nseg, st_, ct, it, c["D"], c["T2"],
+                    dL=tuple(c["dL"]))
+    N, nt, dt = int(c["N"]), int(c["nt"]), float(c["dt"])
+    dirs = c["dirs"].astype(np.float32)
+    x0 = c["x0"].astype(np.float32)
+    spins, spins0 = x0.copy(), x0.copy()
+    phase = np.zeros((dirs.shape[1], N), np.float32)
+    r = oz.walk_f32(g, oz.philox(5), oz.MODE_PHASE, spins, spins0, 0, nt, dt, G=c["G"], Garea=c["Garea"],
+                    phase=phase, diffdir=dirs)
+    x = _dev(x0)
+    wk = eng.Walkers.with_counters(x, x.clone(), phase=torch.zeros((dirs.shape[1], N), device="cuda"),
+                                   diffdir=_dev(dirs))
+    for s in range(nt):
+        eng.walk_step(sub, wk, eng.L.MODE_PHASE, dt, float(c["G"][s]), float(c["Garea"][s]), s, eng.philox_draws(5))
+    np.testing.assert_array_equal(wk.spins.cpu().numpy(), spins)
+    np.testing.assert_array_equal(wk.phase.cpu().numpy(), phase)
+    np.testing.assert_array_equal(wk.n_scatter.cpu().numpy(), r["n_scatter"])
+    np.testing.assert_array_equal(wk.label.cpu().numpy(), r["label"])
+
+
+def test_injected_table_draws(eng):
+    """Injected normal tables, exhaustion included (a drained table reads 0)."""
+    c = load("narrow_chain_out")
+    sub = _sub_from_case(eng, c)
+    N, nt = int(c["N"]), 40
+    rng = np.random.default_rng(3)
+    table = rng.standard_normal((N, nt, 6), dtype=np.float32)  # at most 2 draws per step
+    g = oracle_geometry(c)
+    spins, spins0 = c["x0"].copy(), c["x0"].copy()
+    sig = np.ones(N, np.float32)
+    r = oz.walk_f32(g, oz.injected(table), oz.MODE_SIG, spins, spins0, 0, nt, float(c["dt"]), sig=sig)
+    assert (r["flags"] & oz.FLAG_DRAWS_EXHAUSTED).any()
+    x = _dev(c["x0"])
+    wk = eng.Walkers.with_counters(x, x.clone(), sig=torch.ones(N, device="cuda"))
+    tab = _dev(table)
+    for s in range(nt):
+        eng.walk_step(sub, wk, eng.L.MODE_SIG, float(c["dt"]), 0.0, 0.0, s, eng.injected_draws(tab))
+    np.testing.assert_array_equal(wk.spins.cpu().numpy(), spins)
+    np.testing.assert_array_equal(wk.flags.cpu().numpy(), r["flags"])
+    np.testing.assert_array_equal(wk.n_scatter.cpu().numpy(), r["n_scatter"])
+
+
+def test_seeding_matches_oracle(eng):
+    c = load("dwi_overlap")
+    sph, L3, nseg = c["spheres"], tuple(c["L"]), tuple(int(v) for v in c["nseg"])
+    sub = eng.DeviceSubstrate(sph, 3, L3, nseg, c["D"], c["T2"])
+    st_, ct, it = cells_members(sph, L3, nseg)
+    g = oz.Geometry(sph.astype(np.float32), 3, L3, nseg, st_, ct, it, c["D"], c["T2"], dL=tuple(c["dL"]))
+    for targets in ([0, 1, 2], [3], [1], [0, 1, 2, 3]):
+        spins, label = eng.seed(sub, targets, 5000, key=77)
+        ref_spins, ref_label, left = oz.seed(g, targets, 5000, key0=77, key1=0, stream=1)
+        assert left == 0
+        np.testing.assert_array_equal(spins.cpu().numpy(), ref_spins)
+        np.testing.assert_array_equal(label.cpu().numpy(), ref_label)
+
+
+def test_seeding_reports_empty_target(eng):
+    sph = np.array([[0.0], [0.0], [0.0], [1e-6], [0.0]])
+    sub = eng.DeviceSubstrate(sph, 1, (10.0, 10.0, 10.0), (1, 1, 1), [2.0, 2.0], [100.0, 100.0])
+    with pytest.raises(eng.NozomiError):
+        eng.seed(sub, [0], 64, key=1, max_rounds=50)
+
+
+def test_signal_and_moments_match_oracle(eng):
+    rng = np.random.default_rng(8)
+    N = 20000
+    phi = rng.normal(0, 3, (6, N)).astype(np.float32)
+    phi[3:] *= 1e-6
+    x = _dev(rng.normal(0, 1, (3, N)).astype(np.float32))
+    wk = eng.Walkers(x, x.clone(), phi=_dev(phi))
+    st = eng.FusedState.from_walkers(wk)
+    dirs = rng.standard_normal((3, 7))
+    dirs /= np.linalg.norm(dirs, axis=0)
+    amps = np.array([0.0, 0.3, 1.0, 2.5])
+    out = st.signal(_dev(dirs.astype(np.float32)), _dev(amps.astype(np.float32)))
+    S = (out[0] + 1j * out[1]).cpu().numpy() / N
+    ref = oz.signal_phi(phi, dirs.astype(np.float32), amps.astype(np.float32))
+    np.testing.assert_allclose(S, ref, atol=1e-6)
+    s0 = rng.normal(0, 1, (3, N)).astype(np.float32)
+    m = torch.zeros(6, dtype=torch.float64, device="cuda")
+    eng.moments(x, _dev(s0), m)
+    np.testing.assert_allclose(m.cpu().numpy(), oz.moments(x.cpu().numpy(), s0), rtol=1e-10)
