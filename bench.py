@@ -1,0 +1,386 @@
+"""Benchmark of the spin random walk: walker-steps/s on the packed-substrate
+workload (200 beaded axons, 20,000 spheres + periodic images, 40x40x80 um box,
+1e6 walkers per GPU, PGSE 20/10/30 ms at dt = 5 us = 6000 steps, 30 directions
+x b in {0, 1, 2, 3} ms/um^2).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One step = one pass of the hot path over one batch: every walker through all
+6000 time steps (fused launches with re-binning between them) plus the signal
+reduction, inputs (seeded positions, substrate, protocol) resident in HBM.
+`value` is the whole-job walker-steps/s (all ranks; walkers are sharded,
+weak scaling, no data-path collective).  `e2e` is the same metric through the
+public call with host buffers: positions copied in from pinned memory and the
+signal copied out every step.
+
+--impl reference: the reference has no CPU implementation of the walk, so the
+reference arm times the oracle (a C/OpenMP restatement of the reference kernel,
+oracle/walk_oracle.c) on the host cores, on a bounded sample of the same
+workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = ("packed substrate: 200 beaded axons x 100 spheres (lognormal r0 1.0/0.3 um, bead amplitude "
+            "U[0.2,0.5]), periodic 40x40x80 um box, 1e6 walkers/GPU over intra+extra space, D=2.0 um^2/ms, "
+            "PGSE delta=10 Delta=20 te=30 ms at dt=5 us (6000 steps), 30 directions x b={0,1,2,3} ms/um^2")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--walkers", type=int, default=1_000_000)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cell", type=float, default=None)
+    ap.add_argument("--steps-per-launch", type=int, default=None)
+    ap.add_argument("--coarsen", type=int, default=None)
+    return ap.parse_args()
+
+
+def workload():
+    from nozomi_b200 import substrates as sb
+    from nozomi_b200.waveforms import PGDiffWaveform
+    sub = sb.packed_axons(seed=2)
+    pg = PGDiffWaveform(20.0, 10.0, 30.0, time_step=0.005)
+    rng = np.random.default_rng(2)
+    dirs = rng.standard_normal((3, 30))
+    dirs /= np.linalg.norm(dirs, axis=0)
+    bvals = np.array([0.0, 1.0, 2.0, 3.0])
+    return sub, pg, dirs, bvals
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle on the host cores
+# ---------------------------------------------------------------------------
+def cpu_sample(sub, pg, dirs, cell, seconds, rank_seed=0, work=True):
+    """Time the oracle on a bounded sample sized to about `seconds` of work.
+    Returns (walker-steps/s, cores, sample description, work per walker-step)."""
+    from oracle import oracle as oz
+    from nozomi_b200.substrates import cell_grid
+    from nozomi_b200.waveforms import step_tables
+    cores = os.cpu_count() or 1
+    sph = sub.spheres()
+    nseg = cell_grid(sub.L, cell)
+    st, ct, it = oz.cells(sph, sub.L, nseg)
+    ns = sub.nstructures
+    g = oz.Geometry(sph.astype(np.float32), ns, sub.L, nseg, st, ct, it, np.full(ns + 1, 2.0, np.float32),
+                    np.full(ns + 1, 100.0, np.float32))
+    G, Ga = step_tables(pg)
+    nw = 64 * cores
+    spins, _, left = oz.seed(g, list(range(ns + 1)), nw, key0=rank_seed ^ 0x5EED)
+    probe_steps = 20
+    sp, s0, phi = spins.copy(), spins.copy(), np.zeros((6, nw), np.float32)
+    t = time.perf_counter()
+    oz.walk_f32(g, oz.philox(rank_seed), oz.MODE_PHI, sp, s0, 0, probe_steps, pg.dt, G=G, Garea=Ga, phi=phi,
+                counters=False, nthreads=cores)
+    rate = nw * probe_steps / (time.perf_counter() - t)
+    nsteps = int(np.clip(seconds * rate / nw, 20, G.size))
+    if nsteps == G.size:  # the whole protocol is short: add walkers instead
+        nw = int(np.clip(seconds * rate / G.size, nw, 4_000_000))
+        spins, _, left = oz.seed(g, list(range(ns + 1)), nw, key0=rank_seed ^ 0x5EED)
+    sp, s0, phi = spins.copy(), spins.copy(), np.zeros((6, nw), np.float32)
+    t = time.perf_counter()
+    oz.walk_f32(g, oz.philox(rank_seed), oz.MODE_PHI, sp, s0, 0, nsteps, pg.dt, G=G, Garea=Ga, phi=phi,
+                counters=False, nthreads=cores)
+    el = time.perf_counter() - t
+    value = nw * nsteps / el
+    wk = None
+    if work:
+        nwk = min(nw, 2048)
+        sp, s0, phi = spins[:, :nwk].copy(), spins[:, :nwk].copy(), np.zeros((6, nwk), np.float32)
+        r = oz.walk_f32(g, oz.philox(rank_seed), oz.MODE_PHI, sp, s0, 0, min(nsteps, 200), pg.dt, G=G, Garea=Ga,
+                        phi=phi, counters=False, work=True, nthreads=cores)
+        n = nwk * min(nsteps, 200)
+        wk = {"iterations": r["work"][0] / n, "spheres_in_reach": r["work"][1] / n, "solves_in_reach": r["work"][2] / n}
+    sample = f"{nw} walkers x {nsteps} steps (steps 0..{nsteps - 1} of the protocol), {el:.1f} s"
+    return value, cores, sample, wk
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sub, pg, dirs, bvals = workload()
+    from oracle.build import build_oracle
+    build_oracle()
+    total_t, total_ws = 0.0, 0
+    value = cores = sample = None
+    for i in range(args.warmup + args.steps):
+        v, cores, sample, _ = cpu_sample(sub, pg, dirs, args.cell or 1.0, args.cpu_seconds / 2, rank_seed=i,
+                                         work=False)
+        if i >= args.warmup:
+            total_ws += 1
+            total_t += 1.0 / v
+            value = v if value is None else value
+    value = total_ws / total_t
+    line = {"impl": "reference", "metric": "walker-steps/s", "value": value, "unit": "walker-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cell_um": args.cell or 1.0},
+            "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": "port",
+                             "sample": sample + "; oracle/walk_oracle.c (C restatement of sim3d_kernel.cu's "
+                                                "walk, OpenMP over walkers)"},
+            "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = Path("/tmp") / f"nz_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = [r.split(", ") for r in self.path.read_text().strip().splitlines() if r.strip()]
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from nozomi_b200 import engine, _lib as L
+    from nozomi_b200.simulate import DwiRun, Tuning, device_substrate
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    engine.require_cuda()
+    sub, pg, dirs, bvals = workload()
+    tuning = Tuning()
+    if args.cell:
+        tuning.cell = args.cell
+    if args.steps_per_launch:
+        tuning.steps_per_launch = args.steps_per_launch
+    if args.coarsen:
+        tuning.coarsen = args.coarsen
+    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell)
+    amps = pg.amplitude_for_b(bvals)
+    N = args.walkers
+    run = DwiRun(dsub, pg, dirs, amps, N, seed=1000 + rank, tuning=tuning)
+    x0 = run.initial_positions()
+    flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def one_step(walk_events=None):
+        run.prepare(x0)
+        t = run.tuning
+        for s0 in range(0, run.nsteps, t.steps_per_launch):
+            run._scratch = run.state.sort_into(run.spare, run.sub.grid, t.coarsen, run._scratch)
+            run.state, run.spare = run.spare, run.state
+            if walk_events is not None:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            engine.walk_fused(run.sub, run.state, L.MODE_PHI, run.dt, run.G, run.Garea, s0,
+                              min(run.nsteps, s0 + t.steps_per_launch), run.draws)
+            if walk_events is not None:
+                e1.record(stream)
+                walk_events.append((e0, e1))
+        return run.signal_sums()
+
+    n_chunks = -(-run.nsteps // tuning.steps_per_launch)
+    # kernels per step: pack, then per chunk (memset-free) bin_count + scan + scatter + walk, then signal
+    launches_per_step = 1 + 4 * n_chunks + 1
+
+    # FP32 peak of this GPU (probe kernel), before the timed region
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    probe_out = torch.zeros(sms * 16, device="cuda")
+    lib = L.load()
+    iters = 4096
+    for _ in range(2):
+        L.check(lib.nz_probe_fma(sms * 16, iters, probe_out.data_ptr(), stream.cuda_stream), "probe")
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record(stream)
+    L.check(lib.nz_probe_fma(sms * 16, iters, probe_out.data_ptr(), stream.cuda_stream), "probe")
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    fp32_peak_tflops = sms * 16 * 256 * iters * 8 * 2 / (pe0.elapsed_time(pe1) * 1e-3) / 1e12
+
+    for _ in range(args.warmup):
+        one_step()
+        flush.zero_()
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    step_ms, walk_ms, n_walk = 0.0, 0.0, 0
+    sig = None
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (outside the step's events)
+        torch.cuda.synchronize()
+        ev = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sig = one_step(ev)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        step_ms += e0.elapsed_time(e1)
+        walk_ms += sum(a.elapsed_time(b) for a, b in ev)
+        n_walk += len(ev)
+    barrier()
+    clk = clocks.stop()
+    t_local = torch.tensor([step_ms, walk_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    step_ms, walk_ms = float(t_local[0]), float(t_local[1])
+    ws_per_step = N * run.nsteps * world
+    value = ws_per_step * args.steps / (step_ms * 1e-3)
+    S = sig.cpu().numpy()
+    S = (S[0] + 1j * S[1]) / N
+
+    # end to end through the public call with host buffers
+    x_host = x0.cpu().pin_memory()
+    e2e_ms = 0.0
+    out_bytes = 0
+    for i in range(args.e2e_steps + 1):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        xd = x_host.to("cuda", non_blocking=True)
+        sig_d = one_step_with(run, xd)
+        host = sig_d.to("cpu")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out_bytes = host.numel() * host.element_size()
+        if i > 0:  # first pass warms the path
+            e2e_ms += e0.elapsed_time(e1)
+    t_local = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    e2e_value = ws_per_step * args.e2e_steps / (float(t_local[0]) * 1e-3)
+
+    line = None
+    if rank == 0:
+        walk_launch_ms = walk_ms / max(n_walk, 1)
+        per_launch_ws = N * tuning.steps_per_launch
+        kernel_ws_s = N * run.nsteps * args.steps / (walk_ms * 1e-3)
+        cpu = None
+        wk = None
+        if world == 1 and not args.no_cpu_baseline:
+            v, cores, sample, wk = cpu_sample(sub, pg, dirs, tuning.cell, args.cpu_seconds)
+            cpu = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "port",
+                   "sample": sample + "; oracle/walk_oracle.c, OpenMP over walkers"}
+        peaks = {}
+        pk = ROOT / "MEASURED_PEAKS.json"
+        if pk.exists():
+            peaks = json.loads(pk.read_text())
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        # HBM view: walker state read + written once per launch (4 x float4 each way)
+        state_bytes = N * 128
+        roof_hbm = {"bound": "hbm", "achieved": state_bytes / (walk_launch_ms * 1e-3) / 1e9, "peak": hbm_peak,
+                    "unit": "GB/s", "traffic": None,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk.exists() else "fallback 6.65 TB/s"}
+        roof_hbm["frac"] = roof_hbm["achieved"] / hbm_peak
+        roof_fp32 = None
+        if wk is not None:
+            F_alg = 10 * wk["spheres_in_reach"] + 36 * wk["solves_in_reach"] + 6 * dirs.shape[1]
+            ach = kernel_ws_s * F_alg / 1e12
+            roof_fp32 = {"bound": "fp32", "achieved": ach, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
+                         "frac": ach / fp32_peak_tflops, "flops_per_walker_step": F_alg, "work_per_walker_step": wk,
+                         "peak_source": "nz_probe_fma on this GPU (8 FFMA chains/thread)"}
+        line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded packed-axon substrate, seeded walkers)",
+                "config": {"workload": WORKLOAD, "walkers_per_gpu": N, "time_steps": run.nsteps,
+                           "directions": int(dirs.shape[1]), "bvalues": bvals.tolist(),
+                           "cell_um": tuning.cell, "steps_per_launch": tuning.steps_per_launch,
+                           "rebin_coarsen": tuning.coarsen, "spheres": sub.S, "cells": dsub.ncell,
+                           "cell_list_entries": dsub.n_items, "l2": "256 MiB flush between timed steps",
+                           "parallelism": f"walkers sharded over {world} GPU(s)"},
+                "e2e": {"value": e2e_value, "unit": "walker-steps/s",
+                        "h2d_bytes_per_step": int(x_host.numel() * x_host.element_size()),
+                        "d2h_bytes_per_step": int(out_bytes)},
+                "gpu_launches": launches_per_step * args.steps,
+                "kernel": {"name": "walk_fused_kernel", "launches": n_walk, "avg_launch_ms": walk_launch_ms,
+                           "walker_steps_per_launch": per_launch_ws, "kernel_walker_steps_per_s": kernel_ws_s,
+                           "share_of_step": walk_ms / step_ms},
+                "roofline": roof_hbm, "roofline_fp32": roof_fp32, "cpu_baseline": cpu, "clocks": clk,
+                "signal_b0_mean": float(np.mean(np.abs(S[:, 0]))),
+                "signal_mean_by_b": [float(np.mean(S[:, b].real)) for b in range(S.shape[1])]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def one_step_with(run, x):
+    from nozomi_b200 import engine, _lib as L
+    run.prepare(x)
+    t = run.tuning
+    for s0 in range(0, run.nsteps, t.steps_per_launch):
+        run._scratch = run.state.sort_into(run.spare, run.sub.grid, t.coarsen, run._scratch)
+        run.state, run.spare = run.spare, run.state
+        engine.walk_fused(run.sub, run.state, L.MODE_PHI, run.dt, run.G, run.Garea, s0,
+                          min(run.nsteps, s0 + t.steps_per_launch), run.draws)
+    return run.signal_sums()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

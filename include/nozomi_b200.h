@@ -217,6 +217,11 @@ int nz_phase_from_phi(const nz_state* st, const float* dirs, int ndir, float* ph
  * divisions: out[6] += (sum dx^2, dy^2, dz^2, dx^4, dy^4, dz^4), FP64. ---- */
 int nz_moments(const float* spins, const float* spins0, int N, double* out, void* stream);
 
+/* ---- measurement aid (no reference counterpart): FP32 fused multiply-add
+ * throughput of this GPU, grid x 256 threads x iters x 8 FMAs; the benchmark
+ * divides its FP32 work by this peak. ---- */
+int nz_probe_fma(int grid, int iters, float* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,7 @@ SIGNATURES = {
     "nz_signal_phi": (_i, [_P, _P, _i, _P, _i, _P, _P]),
     "nz_phase_from_phi": (_i, [_P, _P, _i, _P, _P]),
     "nz_moments": (_i, [_P, _P, _i, _P, _P]),
+    "nz_probe_fma": (_i, [_i, _i, _P, _P]),
 }
 
 _lib = None

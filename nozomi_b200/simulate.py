@@ -1,0 +1,122 @@
+"""The fused production path of one substrate: seed, walk every step of a
+protocol in a few launches with walkers re-binned by cell between them, and
+reduce the signal on the device.
+
+This is the work of DwiSim3d.simulate_multi_directions
+(simulation_toolkit/simulation_engine/diffsim3d.py:246-261, one kernel launch
+per waveform sample) plus the signal reduction the reference leaves to the
+caller, and of the narrow-pulse loop of cli/simulation_main.py:91-118 (walk
+plus one moment kernel per step).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import engine
+from . import _lib as L
+from .substrates import Substrate, cell_grid
+from .waveforms import step_tables
+
+
+@dataclass
+class Tuning:
+    """Launch shape of the fused walk (chosen by nozomi_b200.autotune)."""
+    cell: float = 1.0             # cell edge, um
+    steps_per_launch: int = 500   # steps between walker re-binnings
+    coarsen: int = 2              # re-binning bins = cells coarsened by this factor per axis
+
+
+def device_substrate(sub: Substrate, D=2.0, T2=100.0, cell: float = 1.0, nseg=None, D_box=None,
+                     jump_tol: float = 1.0) -> engine.DeviceSubstrate:
+    nseg = cell_grid(sub.L, cell) if nseg is None else nseg
+    ns = sub.nstructures
+    Dv = np.full(ns + 1, D, np.float32)
+    if D_box is not None:
+        Dv[ns] = D_box
+    T2v = np.full(ns + 1, T2, np.float32)
+    return engine.DeviceSubstrate(sub.spheres(), ns, sub.L, nseg, Dv, T2v, jump_tol=jump_tol)
+
+
+class DwiRun:
+    """Walkers of one substrate under one gradient waveform; signal for every
+    (direction, amplitude) pair of the unit-amplitude waveform (phase is linear
+    in the gradient: phi(a) = a * phi(1))."""
+
+    def __init__(self, dsub: engine.DeviceSubstrate, gwave, dirs: np.ndarray, amplitudes, N: int, seed: int = 0,
+                 targets=None, tuning: Tuning | None = None, positions: torch.Tensor | None = None):
+        self.sub = dsub
+        self.tuning = tuning or Tuning()
+        self.dt = float(gwave.dt)
+        G, Ga = step_tables(gwave)
+        self.nsteps = G.size
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.G = torch.from_numpy(G).to(dev)
+        self.Garea = torch.from_numpy(Ga).to(dev)
+        d = np.asarray(dirs, np.float64)
+        if d.ndim != 2 or d.shape[0] != 3:
+            raise TypeError("dirs must be a 3 x ndir array")
+        self.dirs = torch.from_numpy(d.astype(np.float32)).to(dev)
+        self.amps = torch.as_tensor(np.asarray(amplitudes, np.float32).ravel(), device=dev)
+        self.N = int(N)
+        self.seed = int(seed)
+        self.targets = list(range(dsub.nstructures + 1)) if targets is None else list(targets)
+        self.draws = engine.philox_draws(self.seed, 0)
+        self.positions = positions
+        self._scratch = None
+        self.launches = 0
+
+    def initial_positions(self) -> torch.Tensor:
+        if self.positions is not None:
+            return self.positions
+        spins, _ = engine.seed(self.sub, self.targets, self.N, key=self.seed ^ 0x5EED)
+        return spins
+
+    def prepare(self, positions: torch.Tensor | None = None):
+        x = self.initial_positions() if positions is None else positions
+        N = x.shape[1]
+        wk = engine.Walkers(x, x.clone(), phi=torch.zeros((6, N), device=x.device))
+        self.state = engine.FusedState.from_walkers(wk)
+        self.spare = engine.FusedState(N)
+        return self
+
+    def walk(self):
+        t = self.tuning
+        self.launches = 0
+        for s0 in range(0, self.nsteps, t.steps_per_launch):
+            self._scratch = self.state.sort_into(self.spare, self.sub.grid, t.coarsen, self._scratch)
+            self.state, self.spare = self.spare, self.state
+            engine.walk_fused(self.sub, self.state, L.MODE_PHI, self.dt, self.G, self.Garea, s0,
+                              min(self.nsteps, s0 + t.steps_per_launch), self.draws)
+            self.launches += 4
+        return self
+
+    def signal_sums(self) -> torch.Tensor:
+        """[2, ndir, nb] float64 sums over walkers of cos / sin."""
+        out = self.state.signal(self.dirs, self.amps)
+        self.launches += 1
+        return out
+
+    def signal(self) -> np.ndarray:
+        s = self.signal_sums().cpu().numpy()
+        return (s[0] + 1j * s[1]) / self.state.N
+
+    def phase(self) -> torch.Tensor:
+        """Per-walker phase [ndir, N] of the unit waveform, walker-id order."""
+        order = torch.argsort(self.state.walker_ids())
+        return self.state.phase(self.dirs)[:, order]
+
+
+def simulate_dwi(sub: Substrate, gwave, dirs, bvalues=None, amplitudes=None, N: int = 100000, D=2.0, T2=100.0,
+                 seed: int = 0, targets=None, tuning: Tuning | None = None) -> np.ndarray:
+    """Signal S[d][b] of a substrate under gwave, along dirs, for b-values
+    (ms/um^2) or wave amplitudes (units of 100 mT/m)."""
+    engine.require_cuda()
+    if amplitudes is None:
+        amplitudes = gwave.amplitude_for_b(bvalues)
+    tuning = tuning or Tuning()
+    dsub = device_substrate(sub, D=D, T2=T2, cell=tuning.cell)
+    run = DwiRun(dsub, gwave, dirs, amplitudes, N, seed=seed, targets=targets, tuning=tuning).prepare()
+    return run.walk().signal()

@@ -49,11 +49,29 @@ def lib():
         _lib.oz_moments.argtypes = [i, _P, _P, _P]
         _lib.oz_signal_phi.argtypes = [i, _P, _P, i, _P, i, _P, _P]
         _lib.oz_signal_phase.argtypes = [i, _P, i, _P, i, _P, _P]
+        _lib.oz_cells.argtypes = [_P, i, d, d, d, i, i, i, d, _P, _P, _P]
+        _lib.oz_cells.restype = ctypes.c_longlong
         for fn in ("oz_walk_f32", "oz_walk_f64", "oz_seed"):
             getattr(_lib, fn).restype = ctypes.c_int
         for fn in ("oz_seed_accept", "oz_philox_normals", "oz_moments", "oz_signal_phi", "oz_signal_phase"):
             getattr(_lib, fn).restype = None
     return _lib
+
+
+def cells(spheres64, L, nseg, jump_tol: float = 1.0):
+    """Member cell lists (start, count, items) built on the host in C."""
+    sph = np.ascontiguousarray(spheres64, np.float64)
+    nx, ny, nz = (int(v) for v in nseg)
+    ncell = nx * ny * nz
+    count = np.zeros(ncell, np.int32)
+    start = np.zeros(ncell, np.int32)
+    Lx, Ly, Lz = (float(v) for v in L)
+    total = lib().oz_cells(sph.ctypes.data, sph.shape[1], Lx, Ly, Lz, nx, ny, nz, jump_tol, count.ctypes.data,
+                           start.ctypes.data, None)
+    items = np.zeros(max(int(total), 1), np.int32)
+    lib().oz_cells(sph.ctypes.data, sph.shape[1], Lx, Ly, Lz, nx, ny, nz, jump_tol, count.ctypes.data,
+                   start.ctypes.data, items.ctypes.data)
+    return start, count, items[:int(total)]
 
 
 def _ptr(a):

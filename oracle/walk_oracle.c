@@ -340,3 +340,57 @@ OZ_API void oz_signal_phase(int N, const double* phase, int ndir, const double* 
             }
     for (int i = 0; i < ndir * nb; ++i) { re[i] /= N; im[i] /= N; }
 }
+
+/*
+ * Member cell lists (diffsim3d.py:128-141 predicate, float64, reference
+ * operation order), sphere by sphere over the box of cells each sphere can
+ * belong to.  Two calls: items == NULL fills count[ncell] and returns the
+ * total; otherwise start[] (exclusive scan of count) is filled and items[]
+ * receives each cell's members in ascending index order.
+ */
+static inline double oz_seg_lo(double n, double dL, double r, double x, double L) { return n*dL - r - x - L/2; }
+static inline double oz_seg_hi(double n, double dL, double r, double x, double L) { return x - ((n+1)*dL + r - L/2); }
+
+static void oz_axis_range(double x, double r, double L, int nseg, double tol, int* lo, int* hi) {
+    double dL = L / nseg;
+    int a = (int)floor((x - r + L/2 - tol) / dL) - 2;
+    int b = (int)ceil((tol + r + x + L/2) / dL) + 2;
+    if (a < 0) a = 0;
+    if (b > nseg - 1) b = nseg - 1;
+    *lo = 1; *hi = 0;
+    for (int n = a; n <= b; ++n) {
+        if (oz_seg_lo(n, dL, r, x, L) < tol && oz_seg_hi(n, dL, r, x, L) < tol) {
+            if (*lo > *hi) *lo = n;
+            *hi = n;
+        }
+    }
+}
+
+OZ_API long long oz_cells(const double* sph, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz,
+                          double tol, int* count, int* start, int* items) {
+    const long long ncell = (long long)nx * ny * nz;
+    if (!items) {
+        memset(count, 0, sizeof(int) * ncell);
+    } else {
+        long long acc = 0;
+        for (long long c = 0; c < ncell; ++c) { start[c] = (int)acc; acc += count[c]; }
+        memset(count, 0, sizeof(int) * ncell);
+    }
+    long long total = 0;
+    for (int s = 0; s < S; ++s) {
+        double x = sph[s], y = sph[S + s], z = sph[2*S + s], r = sph[3*S + s];
+        int x0, x1, y0, y1, z0, z1;
+        oz_axis_range(x, r, Lx, nx, tol, &x0, &x1);
+        oz_axis_range(y, r, Ly, ny, tol, &y0, &y1);
+        oz_axis_range(z, r, Lz, nz, tol, &z0, &z1);
+        for (int p = z0; p <= z1; ++p)
+            for (int m = y0; m <= y1; ++m)
+                for (int n = x0; n <= x1; ++n) {
+                    long long c = ((long long)p * ny + m) * nx + n;
+                    if (items) items[start[c] + count[c]] = s;
+                    count[c]++;
+                    total++;
+                }
+    }
+    return total;
+}
