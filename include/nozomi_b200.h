@@ -202,6 +202,18 @@ size_t nz_sort_scratch_bytes(int N, int nbins);
 int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out, void* scratch,
                   size_t scratch_bytes, void* stream);
 
+/* Re-binning for callers that cannot allocate device memory (no counterpart in
+ * the reference, which re-bins nothing).  Same result as nz_state_sort, but the
+ * scratch is a fixed 16 MiB device array inside the library (one per GPU that
+ * loads it, held until exit): no buffer is passed and nothing is allocated.
+ * Fails with NZ_ERR_CAPACITY when nz_sort_scratch_bytes(N, nbins) exceeds
+ * nz_state_sort_static_capacity().  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller. */
+size_t nz_state_sort_static_capacity(void);
+int nz_state_sort_static(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out, void* stream);
+
 /* ---- a13: signal S[d][b] = sum_w exp(i * amp[b] * u_d . Phi_w) over walkers,
  * FP32 per walker, FP64 sums (the reference stops at per-spin phase,
  * diffsim3d.py:257-261).  dirs: [3, ndir]; amp: [nb]; out: [2][ndir][nb] doubles

@@ -75,6 +75,8 @@ SIGNATURES = {
     "nz_walk_batch": (_i, [_P, _i, _P, _i, _i, _i, _i, _P, _i, _P]),
     "nz_sort_scratch_bytes": (ctypes.c_size_t, [_i, _i]),
     "nz_state_sort": (_i, [_P, _P, _i, _P, _P, ctypes.c_size_t, _P]),
+    "nz_state_sort_static_capacity": (ctypes.c_size_t, []),
+    "nz_state_sort_static": (_i, [_P, _P, _i, _P, _P]),
     "nz_signal_phi": (_i, [_P, _P, _i, _P, _i, _P, _P]),
     "nz_phase_from_phi": (_i, [_P, _P, _i, _P, _P]),
     "nz_moments": (_i, [_P, _P, _i, _P, _P]),

@@ -1,5 +1,6 @@
 // Seeding, walker re-binning, signal and moment reductions.
 #include <cstdint>
+#include <mutex>
 #include "kernels.cuh"
 
 namespace nz {
@@ -252,4 +253,58 @@ extern "C" int nz_moments(const float* spins, const float* spins0, int N, double
   if (N == 0) return NZ_OK;
   moments_kernel<<<(N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(spins, spins0, N, out);
   return check_launch("moments_kernel");
+}
+
+// ---------------------------------------------------------------------------
+// Re-binning without caller-provided scratch.  Some hosts cannot hand this
+// library a device buffer: their memory manager reserves all device memory
+// at start-up and forbids allocation afterwards, or an allocation's implicit
+// synchronisation would stall their other streams.  For them the sort's
+// scratch lives in a fixed device array of this file, one copy per GPU that
+// loads the library, kept until the process exits.
+// ---------------------------------------------------------------------------
+namespace nz {
+constexpr size_t kStaticSortScratch = size_t(16) << 20;  // 16 MiB per GPU
+static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortScratch];
+
+// Device address of g_sort_scratch on the current device, looked up once per
+// device (the host-side name of a __device__ array is not a device address).
+static int static_sort_scratch(void** out) {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static void* addr[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_launch("nz_state_sort_static: cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return set_error(NZ_ERR_ARG, "nz_state_sort_static: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess)
+      return set_error(NZ_ERR_CUDA, "nz_state_sort_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return NZ_OK;
+}
+}  // namespace nz
+
+extern "C" size_t nz_state_sort_static_capacity(void) { return kStaticSortScratch; }
+
+extern "C" int nz_state_sort_static(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out,
+                                    void* stream) {
+  if (!in || !grid || coarsen <= 0) return set_error(NZ_ERR_ARG, "nz_state_sort_static: bad arguments");
+  const long long nbins = 1ll * ((grid->nx + coarsen - 1) / coarsen) * ((grid->ny + coarsen - 1) / coarsen) *
+                          ((grid->nz + coarsen - 1) / coarsen);
+  if (in->N < 0 || nbins > (1 << 26)) return set_error(NZ_ERR_ARG, "nz_state_sort_static: bad sizes");
+  const size_t need = nz_sort_scratch_bytes(in->N, int(nbins));
+  if (need > kStaticSortScratch)
+    return set_error(NZ_ERR_CAPACITY,
+                     "nz_state_sort_static: %d walkers and %lld bins need %zu bytes of scratch, more than the "
+                     "fixed %zu; use nz_state_sort with a caller buffer or coarsen the bins",
+                     in->N, nbins, need, kStaticSortScratch);
+  void* scratch = nullptr;
+  const int rc = static_sort_scratch(&scratch);
+  if (rc != NZ_OK) return rc;
+  return nz_state_sort(in, grid, coarsen, out, scratch, kStaticSortScratch, stream);
 }
