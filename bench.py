@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--cell", type=float, default=None)
     ap.add_argument("--steps-per-launch", type=int, default=None)
     ap.add_argument("--coarsen", type=int, default=None)
+    ap.add_argument("--by-label", type=int, default=None, help="re-bin by (label, bin): 1, or by bin only: 0")
     return ap.parse_args()
 
 
@@ -208,11 +209,13 @@ def run_ours(args):
         tuning.steps_per_launch = args.steps_per_launch
     if args.coarsen:
         tuning.coarsen = args.coarsen
+    if args.by_label is not None:
+        tuning.by_label = bool(args.by_label)
     dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell)
     amps = pg.amplitude_for_b(bvals)
     N = args.walkers
     run = DwiRun(dsub, pg, dirs, amps, N, seed=1000 + rank, tuning=tuning)
-    x0 = run.initial_positions()
+    x0, lab0 = run.initial_positions()
     flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     stream = torch.cuda.current_stream()
 
@@ -221,20 +224,9 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def one_step(walk_events=None):
-        run.prepare(x0)
-        t = run.tuning
-        for s0 in range(0, run.nsteps, t.steps_per_launch):
-            run._scratch = run.state.sort_into(run.spare, run.sub.grid, t.coarsen, run._scratch)
-            run.state, run.spare = run.spare, run.state
-            if walk_events is not None:
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-            engine.walk_fused(run.sub, run.state, L.MODE_PHI, run.dt, run.G, run.Garea, s0,
-                              min(run.nsteps, s0 + t.steps_per_launch), run.draws)
-            if walk_events is not None:
-                e1.record(stream)
-                walk_events.append((e0, e1))
+    def one_step(walk_events=None, x=None):
+        run.prepare(x0 if x is None else x, lab0)
+        run.walk(walk_events)
         return run.signal_sums()
 
     n_chunks = -(-run.nsteps // tuning.steps_per_launch)
@@ -295,7 +287,7 @@ def run_ours(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         xd = x_host.to("cuda", non_blocking=True)
-        sig_d = one_step_with(run, xd)
+        sig_d = one_step(x=xd)
         host = sig_d.to("cpu")
         e1.record(stream)
         torch.cuda.synchronize()
@@ -343,7 +335,7 @@ def run_ours(args):
                 "config": {"workload": WORKLOAD, "walkers_per_gpu": N, "time_steps": run.nsteps,
                            "directions": int(dirs.shape[1]), "bvalues": bvals.tolist(),
                            "cell_um": tuning.cell, "steps_per_launch": tuning.steps_per_launch,
-                           "rebin_coarsen": tuning.coarsen, "spheres": sub.S, "cells": dsub.ncell,
+                           "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label, "spheres": sub.S, "cells": dsub.ncell,
                            "cell_list_entries": dsub.n_items, "l2": "256 MiB flush between timed steps",
                            "parallelism": f"walkers sharded over {world} GPU(s)"},
                 "e2e": {"value": e2e_value, "unit": "walker-steps/s",
@@ -361,18 +353,6 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
-
-
-def one_step_with(run, x):
-    from nozomi_b200 import engine, _lib as L
-    run.prepare(x)
-    t = run.tuning
-    for s0 in range(0, run.nsteps, t.steps_per_launch):
-        run._scratch = run.state.sort_into(run.spare, run.sub.grid, t.coarsen, run._scratch)
-        run.state, run.spare = run.spare, run.state
-        engine.walk_fused(run.sub, run.state, L.MODE_PHI, run.dt, run.G, run.Garea, s0,
-                          min(run.nsteps, s0 + t.steps_per_launch), run.draws)
-    return run.signal_sums()
 
 
 def main():

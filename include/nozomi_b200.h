@@ -63,7 +63,8 @@ typedef struct nz_substrate {
     const int* cell_start;     /* [ncell] offset of each cell's list in cell_items */
     const int* cell_count;     /* [ncell] */
     const int* cell_items;     /* sphere indices, ascending within a cell */
-    const float* cell_sph4;    /* [n_items][4] cx, cy, cz, r of each list entry (fused walk) */
+    const float* cell_sph4;    /* [n_items][4] cx, cy, cz, r of each list entry, per cell ordered by
+                                  (structure id, sphere index) (fused walk, nz_cells_gather) */
     const int* cell_sid;       /* [n_items] structure id of each list entry (fused walk) */
     const float* D;            /* [nstructures + 1] um^2/ms */
     const float* T2;           /* [nstructures + 1] ms */
@@ -154,10 +155,12 @@ int nz_cells_fill(const double* spheres64, int S, double Lx, double Ly, double L
 int nz_segments_fill(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz,
                      int K, int* segments, void* stream);
 
-/* Denormalised list entries for the fused walk: sph4[k] = (cx, cy, cz, r) and
- * sid[k] = structure id of sphere items[k]. */
-int nz_cells_gather(const float* spheres, int S, const int* items, int n_items, float* sph4, int* sid,
-                    void* stream);
+/* List entries of the fused walk: the entries of cell c at
+ * [cell_start[c], cell_start[c] + cell_count[c]) hold the sphere records
+ * sph4 = (cx, cy, cz, r) and structure ids sid of that cell's members
+ * (items), ordered by (structure id, sphere index). */
+int nz_cells_gather(const float* spheres, int S, const int* items, int n_items, const int* cell_start,
+                    const int* cell_count, int ncell, float* sph4, int* sid, void* stream);
 
 /* ---- a7: seeding — seedSpinsKernel (sim3d_kernel.cu:240-337) + SimGeometry3D.gpu_seed
  * (geometry.py:73-174).  target[k] != 0 marks structure k (k = nstructures is the
@@ -201,6 +204,12 @@ int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_it
 size_t nz_sort_scratch_bytes(int N, int nbins);
 int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out, void* scratch,
                   size_t scratch_bytes, void* stream);
+/* As nz_state_sort with the key (label, bin) when nlabels > 0: walkers of one
+ * structure (label in pos.w; out-of-range labels count as nlabels - 1) are
+ * contiguous, ordered by bin within.  Scratch: nz_sort_scratch_bytes(N,
+ * nbins * nlabels). */
+int nz_state_sort_keyed(const nz_state* in, const nz_grid* grid, int coarsen, int nlabels, nz_state* out,
+                        void* scratch, size_t scratch_bytes, void* stream);
 
 /* Re-binning for callers that cannot allocate device memory (no counterpart in
  * the reference, which re-bins nothing).  Same result as nz_state_sort, but the

@@ -66,7 +66,7 @@ SIGNATURES = {
     "nz_exclusive_scan_i32": (_i, [_P, _P, _i, _P, _P]),
     "nz_cells_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _d, _P, _P, _P, _P, _P]),
     "nz_segments_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _i, _P, _P]),
-    "nz_cells_gather": (_i, [_P, _i, _P, _i, _P, _P, _P]),
+    "nz_cells_gather": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _P, _P]),
     "nz_seed": (_i, [_P, _P, _i, _u, _u, _u, _i, _P, _P, _P, _P]),
     "nz_walk_step": (_i, [_P, _P, _i, _f, _f, _f, _i, _P, _P]),
     "nz_state_pack": (_i, [_P, _P, _P, _P]),
@@ -75,6 +75,7 @@ SIGNATURES = {
     "nz_walk_batch": (_i, [_P, _i, _P, _i, _i, _i, _i, _P, _i, _P]),
     "nz_sort_scratch_bytes": (ctypes.c_size_t, [_i, _i]),
     "nz_state_sort": (_i, [_P, _P, _i, _P, _P, ctypes.c_size_t, _P]),
+    "nz_state_sort_keyed": (_i, [_P, _P, _i, _i, _P, _P, ctypes.c_size_t, _P]),
     "nz_state_sort_static_capacity": (ctypes.c_size_t, []),
     "nz_state_sort_static": (_i, [_P, _P, _i, _P, _P]),
     "nz_signal_phi": (_i, [_P, _P, _i, _P, _i, _P, _P]),

@@ -215,13 +215,61 @@ __global__ void __launch_bounds__(256) segments_fill_kernel(const double* __rest
   }
 }
 
-__global__ void cells_gather_kernel(const float* __restrict__ spheres, int S, const int* __restrict__ items, int n,
-                                    float4* __restrict__ sph4, int* __restrict__ sid) {
+// Fused-walk list entries, three passes: (1) each entry gets its structure id
+// and, parked in .x, its sphere index; (2) each cell's entries are sorted by
+// (structure id, sphere index) with a heapsort in place; (3) each entry gets
+// its sphere record.  Sorted by structure id, a walker labelled L may stop at
+// the first entry of a higher structure.
+__global__ void gather_ids_kernel(const float* __restrict__ spheres, int S, const int* __restrict__ items, int n,
+                                  float4* __restrict__ sph4, int* __restrict__ sid) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int s = items[k];
-  sph4[k] = make_float4(spheres[s], spheres[S + s], spheres[2 * S + s], spheres[3 * S + s]);
   sid[k] = int(spheres[4 * S + s]);
+  sph4[k].x = __int_as_float(s);
+}
+
+__global__ void gather_sort_kernel(const int* __restrict__ start, const int* __restrict__ count, int ncell,
+                                   float4* __restrict__ sph4, int* __restrict__ sid) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int base = start[c], n = count[c];
+  auto key = [&](int i) {
+    return (static_cast<unsigned long long>(static_cast<unsigned>(sid[base + i])) << 32) |
+           static_cast<unsigned>(__float_as_int(sph4[base + i].x));
+  };
+  auto swap = [&](int i, int j) {
+    const int t = sid[base + i];
+    sid[base + i] = sid[base + j];
+    sid[base + j] = t;
+    const float u = sph4[base + i].x;
+    sph4[base + i].x = sph4[base + j].x;
+    sph4[base + j].x = u;
+  };
+  auto sift = [&](int root, int end) {
+    while (2 * root + 1 < end) {
+      int child = 2 * root + 1;
+      if (child + 1 < end && key(child) < key(child + 1)) child++;
+      if (key(root) < key(child)) {
+        swap(root, child);
+        root = child;
+      } else {
+        return;
+      }
+    }
+  };
+  for (int i = n / 2 - 1; i >= 0; --i) sift(i, n);
+  for (int end = n - 1; end > 0; --end) {
+    swap(0, end);
+    sift(0, end);
+  }
+}
+
+__global__ void gather_records_kernel(const float* __restrict__ spheres, int S, int n, float4* __restrict__ sph4) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int s = __float_as_int(sph4[k].x);
+  sph4[k] = make_float4(spheres[s], spheres[S + s], spheres[2 * S + s], spheres[3 * S + s]);
 }
 
 // Single-CTA exclusive scan (1024 threads, 8 items per thread per pass).
@@ -322,13 +370,21 @@ extern "C" int nz_segments_fill(const double* spheres64, int S, double Lx, doubl
   return check_launch("segments_fill_kernel");
 }
 
-extern "C" int nz_cells_gather(const float* spheres, int S, const int* items, int n_items, float* sph4, int* sid,
-                               void* stream) {
-  if (S < 0 || n_items < 0 || (n_items > 0 && (!spheres || !items || !sph4 || !sid)))
+extern "C" int nz_cells_gather(const float* spheres, int S, const int* items, int n_items, const int* cell_start,
+                               const int* cell_count, int ncell, float* sph4, int* sid, void* stream) {
+  if (S < 0 || n_items < 0 || ncell < 0 ||
+      (n_items > 0 && (!spheres || !items || !sph4 || !sid || !cell_start || !cell_count)))
     return set_error(NZ_ERR_ARG, "nz_cells_gather: bad arguments");
   if (reinterpret_cast<uintptr_t>(sph4) % 16 != 0) return set_error(NZ_ERR_ARG, "nz_cells_gather: sph4 not 16-byte aligned");
   if (n_items == 0) return NZ_OK;
-  cells_gather_kernel<<<(n_items + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      spheres, S, items, n_items, reinterpret_cast<float4*>(sph4), sid);
-  return check_launch("cells_gather_kernel");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float4* s4 = reinterpret_cast<float4*>(sph4);
+  gather_ids_kernel<<<(n_items + 255) / 256, 256, 0, st>>>(spheres, S, items, n_items, s4, sid);
+  int rc = check_launch("gather_ids_kernel");
+  if (rc) return rc;
+  gather_sort_kernel<<<(ncell + 127) / 128, 128, 0, st>>>(cell_start, cell_count, ncell, s4, sid);
+  rc = check_launch("gather_sort_kernel");
+  if (rc) return rc;
+  gather_records_kernel<<<(n_items + 255) / 256, 256, 0, st>>>(spheres, S, n_items, s4);
+  return check_launch("gather_records_kernel");
 }

@@ -39,6 +39,14 @@ __global__ void walk_plain_kernel(const PlainArgs a);
 
 // ---- fused walk (walk_fused.cu) ----
 constexpr int kFusedThreads = 128;
+#ifndef NZ_FUSED_MIN_BLOCKS
+#define NZ_FUSED_MIN_BLOCKS 6
+#endif
+#ifndef NZ_SCAN_BATCH
+#define NZ_SCAN_BATCH 4
+#endif
+constexpr int kFusedMinBlocks = NZ_FUSED_MIN_BLOCKS;  // CTAs per SM the register budget is sized for
+constexpr int kScanBatch = NZ_SCAN_BATCH;             // cell-list entries loaded together per thread
 constexpr int kMomentSteps = 256;  // steps per launch in NZ_MODE_MOMENTS (shared-memory staging)
 
 struct JobDev {

@@ -38,32 +38,52 @@ struct ScanOut {
 };
 
 // One pass over a cell's list under assumed label L.  Returns false when the
-// walker's label is not L (then nothing in `o` is used).
+// walker's label is not L (then nothing in `o` is used).  The entries of a
+// cell are ordered by structure id: the pass ends at the first entry of a
+// structure above L (the reference skips those spheres, :805-806).  Entries
+// are read kScanBatch at a time so that several loads are in flight per thread.
 __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const int* __restrict__ sid, int start,
                                           int count, int nstructures, float x, float y, float z, int L, float a,
                                           float jx, float jy, float jz, float reach, ScanOut& o) {
   o.fin = 0.0f;
   o.fout = kBig;
   o.any_in = false;
-  bool found = false, lower = false;
+  bool found = false, lower = false, stop = false;
   const float slack = kTol + reach * 1.02f + 2e-3f;
-  for (int base = 0; base < count; base += 32) {
+  for (int base = 0; base < count && !stop; base += 32) {
     const int m = min(32, count - base);
     uint32_t in_mask = 0u, out_mask = 0u;
-    for (int i = 0; i < m; ++i) {
-      const int k = start + base + i;
-      const int s = __ldg(sid + k);
-      if (s > L) continue;
-      const float4 c = __ldg(sph4 + k);
-      const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
-      const float d2 = dx * dx + dy * dy + dz * dz;
-      if (d2 - c.w * c.w < 0) {
-        in_mask |= 1u << i;
-        if (s < L) lower = true;
-        else found = true;
-      } else if (s < L) {
-        const float t = c.w + slack;
-        if (d2 <= t * t) out_mask |= 1u << i;
+    for (int i0 = 0; i0 < m && !stop; i0 += kScanBatch) {
+      int sv[kScanBatch];
+      float4 cv[kScanBatch];
+#pragma unroll
+      for (int u = 0; u < kScanBatch; ++u) {
+        const int k = start + base + i0 + u;
+        if (i0 + u < m) {
+          sv[u] = __ldg(sid + k);
+          cv[u] = __ldg(sph4 + k);
+        } else {
+          sv[u] = 0x7fffffff;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kScanBatch; ++u) {
+        const int s = sv[u];
+        if (s > L) {
+          stop = true;
+        } else {
+          const float dx = x - cv[u].x, dy = y - cv[u].y, dz = z - cv[u].z;
+          const float d2 = dx * dx + dy * dy + dz * dz;
+          const uint32_t bit = 1u << (i0 + u);
+          if (d2 - cv[u].w * cv[u].w < 0) {
+            in_mask |= bit;
+            if (s < L) lower = true;
+            else found = true;
+          } else if (s < L) {
+            const float t = cv[u].w + slack;
+            if (d2 <= t * t) out_mask |= bit;
+          }
+        }
       }
     }
     uint32_t todo = in_mask | out_mask;
@@ -101,27 +121,47 @@ __device__ __forceinline__ int label_of(const float4* __restrict__ sph4, const i
   return L;
 }
 
+// Draw `draw` of step s scaled by ds.
+__device__ __forceinline__ void jump_of(const JobDev& J, uint32_t wid, int s, int draw, float ds, float& jx, float& jy,
+                                        float& jz) {
+  float n0, n1, n2;
+  philox_normal3(J.key0, J.key1, J.stream, wid, uint32_t(s), uint32_t(draw), n0, n1, n2);
+  jx = ds * n0;
+  jy = ds * n1;
+  jz = ds * n2;
+}
+
+// Steps [s0, s1) of walker w.  Registers hold position, label, Phi and its
+// compensation and the step's jump; the origin (spins0) and the flag word stay
+// in memory and are updated in place on the rare wrap / iteration-cap events
+// (except with moments, which read the origin every step).
 template <int MODE>
 __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1, float* s_mom) {
-  float4 P = J.pos[w];
-  float4 O = J.org[w];
-  float4 F = make_float4(0.f, 0.f, 0.f, 1.f), C = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (MODE & (NZ_MODE_PHI | NZ_MODE_SIG)) F = J.phi[w];
-  C = J.comp[w];
+  constexpr bool kMom = (MODE & NZ_MODE_MOMENTS) != 0;
+  const float4 P = J.pos[w];
   float x = P.x, y = P.y, z = P.z;
   int label = __float_as_int(P.w);
-  float x0 = O.x, y0 = O.y, z0 = O.z;
-  const uint32_t wid = __float_as_uint(O.w);
-  float fx = F.x, fy = F.y, fz = F.z, sig = F.w;
-  float kx = C.x, ky = C.y, kz = C.z;
-  int flags = __float_as_int(C.w);
+  const uint32_t wid = __float_as_uint(J.org[w].w);
+  float fx = 0.f, fy = 0.f, fz = 0.f, sig = 1.f, kx = 0.f, ky = 0.f, kz = 0.f;
+  if (MODE & (NZ_MODE_PHI | NZ_MODE_SIG)) {
+    const float4 F = J.phi[w];
+    fx = F.x; fy = F.y; fz = F.z; sig = F.w;
+  }
+  if (MODE & NZ_MODE_PHI) {
+    const float4 C = J.comp[w];
+    kx = C.x; ky = C.y; kz = C.z;
+  }
+  float x0 = 0.f, y0 = 0.f, z0 = 0.f;
+  if (kMom) {
+    const float4 O = J.org[w];
+    x0 = O.x; y0 = O.y; z0 = O.z;
+  }
   if (label < 0 || label > J.nstructures) label = J.nstructures;
 
   const float dt = J.dt;
   int s = s0;
   int niter = 0, draw = 0, start = 0, count = 0;
   float jr = 1.0f, ds = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
-  float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
   while (s < s1) {
     if (niter == 0) {
       const int cell = cell_of(J.g, x, y, z);
@@ -133,22 +173,17 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     niter++;
     float jc = jr;
     if (niter == 1) {
-      philox_normal3(J.key0, J.key1, J.stream, wid, uint32_t(s), 0u, n0, n1, n2);
-      draw = 1;
       ds = sqrtf(2 * __ldg(J.D + label) * dt);
-      jx = ds * n0;
-      jy = ds * n1;
-      jz = ds * n2;
+      jump_of(J, wid, s, 0, ds, jx, jy, jz);
+      draw = 1;
     }
     float a = jx * jx + jy * jy + jz * jz;
     ScanOut r;
     if (!scan_cell(J.sph4, J.sid, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, sqrtf(a) * jr, r)) {
       label = label_of(J.sph4, J.sid, start, count, J.nstructures, x, y, z);
-      if (niter == 1) {
+      if (niter == 1) {  // the first draw's length depends on the label
         ds = sqrtf(2 * __ldg(J.D + label) * dt);
-        jx = ds * n0;
-        jy = ds * n1;
-        jz = ds * n2;
+        jump_of(J, wid, s, 0, ds, jx, jy, jz);
         a = jx * jx + jy * jy + jz * jz;
       }
       scan_cell(J.sph4, J.sid, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, sqrtf(a) * jr, r);
@@ -161,47 +196,55 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     if (jc < jr) {
       jr = sqrtf(ref_max(0, jr * jr - jc * jc));
       if (MODE & NZ_MODE_SIG) sig *= t2_decay(-jc * jc * dt / __ldg(J.T2 + label));
-      philox_normal3(J.key0, J.key1, J.stream, wid, uint32_t(s), uint32_t(draw), n0, n1, n2);
+      jump_of(J, wid, s, draw, ds, jx, jy, jz);
       draw++;
-      jx = ds * n0;
-      jy = ds * n1;
-      jz = ds * n2;
     } else {
       jr -= jc;
       if (MODE & NZ_MODE_SIG) sig *= t2_decay(-jc * dt / __ldg(J.T2 + label));
     }
     if (!((jr > kTol) && (niter < kMaxIter))) {
-      if (niter >= kMaxIter && jr > kTol) flags |= kFlagIterCap;
+      if (niter >= kMaxIter && jr > kTol) {
+        float4* c = J.comp + w;
+        c->w = __int_as_float(__float_as_int(c->w) | kFlagIterCap);
+      }
       if (MODE & NZ_MODE_PHI) {
         const float G = __ldg(J.G + s);
         kahan_add(fx, kx, G * x);
         kahan_add(fy, ky, G * y);
         kahan_add(fz, kz, G * z);
       }
-      const float Ga = (MODE & NZ_MODE_PHI) ? __ldg(J.Garea + s) : 0.0f;
       const float Lx = J.g.Lx, Ly = J.g.Ly, Lz = J.g.Lz;
-      if (x < -Lx / 2) {
-        x += Lx; x0 += Lx;
-        if (MODE & NZ_MODE_PHI) kahan_add(fx, kx, Lx * Ga);
-      } else if (x > Lx / 2) {
-        x -= Lx; x0 -= Lx;
-        if (MODE & NZ_MODE_PHI) kahan_add(fx, kx, -(Lx * Ga));
+      if (fabsf(x) > Lx / 2 || fabsf(y) > Ly / 2 || fabsf(z) > Lz / 2) {  // rare: a wrap
+        const float Ga = (MODE & NZ_MODE_PHI) ? __ldg(J.Garea + s) : 0.0f;
+        float4 O = kMom ? make_float4(x0, y0, z0, 0.f) : J.org[w];
+        if (x < -Lx / 2) {
+          x += Lx; O.x += Lx;
+          if (MODE & NZ_MODE_PHI) kahan_add(fx, kx, Lx * Ga);
+        } else if (x > Lx / 2) {
+          x -= Lx; O.x -= Lx;
+          if (MODE & NZ_MODE_PHI) kahan_add(fx, kx, -(Lx * Ga));
+        }
+        if (y < -Ly / 2) {
+          y += Ly; O.y += Ly;
+          if (MODE & NZ_MODE_PHI) kahan_add(fy, ky, Ly * Ga);
+        } else if (y > Ly / 2) {
+          y -= Ly; O.y -= Ly;
+          if (MODE & NZ_MODE_PHI) kahan_add(fy, ky, -(Ly * Ga));
+        }
+        if (z < -Lz / 2) {
+          z += Lz; O.z += Lz;
+          if (MODE & NZ_MODE_PHI) kahan_add(fz, kz, Lz * Ga);
+        } else if (z > Lz / 2) {
+          z -= Lz; O.z -= Lz;
+          if (MODE & NZ_MODE_PHI) kahan_add(fz, kz, -(Lz * Ga));
+        }
+        if (kMom) {
+          x0 = O.x; y0 = O.y; z0 = O.z;
+        } else {
+          J.org[w] = O;
+        }
       }
-      if (y < -Ly / 2) {
-        y += Ly; y0 += Ly;
-        if (MODE & NZ_MODE_PHI) kahan_add(fy, ky, Ly * Ga);
-      } else if (y > Ly / 2) {
-        y -= Ly; y0 -= Ly;
-        if (MODE & NZ_MODE_PHI) kahan_add(fy, ky, -(Ly * Ga));
-      }
-      if (z < -Lz / 2) {
-        z += Lz; z0 += Lz;
-        if (MODE & NZ_MODE_PHI) kahan_add(fz, kz, Lz * Ga);
-      } else if (z > Lz / 2) {
-        z -= Lz; z0 -= Lz;
-        if (MODE & NZ_MODE_PHI) kahan_add(fz, kz, -(Lz * Ga));
-      }
-      if (MODE & NZ_MODE_MOMENTS) {
+      if (kMom) {
         const float ex = x - x0, ey = y - y0, ez = z - z0;
         float* m = s_mom + 6 * (s - s0);
         const float ex2 = ex * ex, ey2 = ey * ey, ez2 = ez * ez;
@@ -217,9 +260,31 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     }
   }
   J.pos[w] = make_float4(x, y, z, __int_as_float(label));
-  J.org[w] = make_float4(x0, y0, z0, O.w);
+  if (kMom) J.org[w] = make_float4(x0, y0, z0, __uint_as_float(wid));
   if (MODE & (NZ_MODE_PHI | NZ_MODE_SIG)) J.phi[w] = make_float4(fx, fy, fz, sig);
-  J.comp[w] = make_float4(kx, ky, kz, __int_as_float(flags));
+  if (MODE & NZ_MODE_PHI) {
+    float4* c = J.comp + w;
+    *c = make_float4(kx, ky, kz, c->w);
+  }
+}
+
+// One work item: walkers [first, first + count) of job J, steps [step0, step1)
+// clamped to the job's protocol.
+template <int MODE>
+__device__ __forceinline__ void run_item(const JobDev& J, int first, int count, int step0, int step1, float* s_mom) {
+  const int s0 = step0, s1 = min(step1, J.nsteps);
+  if (MODE & NZ_MODE_MOMENTS) {
+    for (int i = threadIdx.x; i < kMomentSteps * 6; i += blockDim.x) s_mom[i] = 0.0f;
+    __syncthreads();
+  }
+  if (threadIdx.x < count && s0 < s1) walk_one<MODE>(J, first + threadIdx.x, s0, s1, s_mom);
+  if (MODE & NZ_MODE_MOMENTS) {
+    __syncthreads();
+    if (J.moments)
+      for (int i = threadIdx.x; i < (s1 - s0) * 6; i += blockDim.x)
+        atomicAdd(J.moments + size_t(s0) * 6 + i, double(s_mom[i]));
+    __syncthreads();
+  }
 }
 
 // Work items are CTAs' worth of walkers of one job.  SINGLE: one job passed by
@@ -227,11 +292,12 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
 // device arrays; with queue != null the grid is persistent and each CTA takes
 // items from *queue until none is left.
 template <int MODE, bool SINGLE>
-__global__ void __launch_bounds__(kFusedThreads) walk_fused_kernel(const JobDev single, const nz_job* __restrict__ jobs,
-                                                                   const nz_item* __restrict__ items, int n_items,
-                                                                   int step0, int step1, int* queue) {
+__global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
+    walk_fused_kernel(const __grid_constant__ JobDev single, const nz_job* __restrict__ jobs,
+                      const nz_item* __restrict__ items, int n_items, int step0, int step1, int* queue) {
   __shared__ int s_item;
   __shared__ float s_mom[(MODE & NZ_MODE_MOMENTS) ? kMomentSteps * 6 : 1];
+  __shared__ JobDev s_job;
   int it = blockIdx.x;
   for (;;) {
     if (queue) {
@@ -241,29 +307,20 @@ __global__ void __launch_bounds__(kFusedThreads) walk_fused_kernel(const JobDev 
       __syncthreads();
     }
     if (it >= n_items) return;
-    nz_item wi;
-    JobDev J;
     if (SINGLE) {
-      J = single;
-      wi.job = 0;
-      wi.first = it * kFusedThreads;
-      wi.count = min(kFusedThreads, J.nwalkers - wi.first);
+      const int first = it * kFusedThreads;
+      const int count = min(kFusedThreads, single.nwalkers - first);
+      run_item<MODE>(single, first, count, step0, step1, s_mom);
     } else {
-      wi = items[it];
-      const nz_job& a = jobs[wi.job];
-      J = make_job(a.sub, a.G, a.Garea, a.nsteps, a.dt, a.draws, a.mode, a.state, a.moments);
-    }
-    const int s0 = step0, s1 = min(step1, J.nsteps);
-    if (MODE & NZ_MODE_MOMENTS) {
-      for (int i = threadIdx.x; i < kMomentSteps * 6; i += blockDim.x) s_mom[i] = 0.0f;
+      // every thread of the CTA works on the same job: its descriptor lives
+      // in shared memory, not in each thread's registers
+      const nz_item wi = items[it];
+      if (threadIdx.x == 0) {
+        const nz_job& a = jobs[wi.job];
+        s_job = make_job(a.sub, a.G, a.Garea, a.nsteps, a.dt, a.draws, a.mode, a.state, a.moments);
+      }
       __syncthreads();
-    }
-    if (threadIdx.x < wi.count && s0 < s1) walk_one<MODE>(J, wi.first + threadIdx.x, s0, s1, s_mom);
-    if (MODE & NZ_MODE_MOMENTS) {
-      __syncthreads();
-      if (J.moments)
-        for (int i = threadIdx.x; i < (s1 - s0) * 6; i += blockDim.x)
-          atomicAdd(J.moments + size_t(s0) * 6 + i, double(s_mom[i]));
+      run_item<MODE>(s_job, wi.first, wi.count, step0, step1, s_mom);
       __syncthreads();
     }
     if (!queue) return;
@@ -343,6 +400,13 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
 template <int MODE>
 void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0, int step1,
                  int* queue, int grid, cudaStream_t st) {
+  // the kernel keeps no data in shared memory: give the whole carveout to L1
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(walk_fused_kernel<MODE, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(walk_fused_kernel<MODE, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    configured = true;
+  }
   if (jobs)
     walk_fused_kernel<MODE, false><<<grid, kFusedThreads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
   else

@@ -61,6 +61,7 @@ struct BinGrid {
   Grid g;
   int cx, cy, cz;     // coarsening per axis
   int bx, by, bz;     // bins per axis
+  int nlabels;        // > 0: key = label * nbins + bin (walkers of one structure together)
 };
 
 __device__ __forceinline__ int bin_of(const BinGrid& b, float x, float y, float z) {
@@ -75,7 +76,12 @@ __global__ void bin_count_kernel(const float4* __restrict__ pos, int N, BinGrid 
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= N) return;
   const float4 p = pos[w];
-  const int k = bin_of(b, p.x, p.y, p.z);
+  int k = bin_of(b, p.x, p.y, p.z);
+  if (b.nlabels > 0) {
+    int label = __float_as_int(p.w);
+    if (label < 0 || label >= b.nlabels) label = b.nlabels - 1;
+    k += label * (b.bx * b.by * b.bz);
+  }
   bins[w] = k;
   atomicAdd(hist + k, 1);
 }
@@ -198,9 +204,9 @@ extern "C" size_t nz_sort_scratch_bytes(int N, int nbins) {
   return align256(size_t(N) * sizeof(int)) + 2 * align256(size_t(nbins) * sizeof(int));
 }
 
-extern "C" int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out, void* scratch,
-                             size_t scratch_bytes, void* stream) {
-  if (!in || !grid || !out || coarsen <= 0 || in->N != out->N || !scratch)
+extern "C" int nz_state_sort_keyed(const nz_state* in, const nz_grid* grid, int coarsen, int nlabels, nz_state* out,
+                                   void* scratch, size_t scratch_bytes, void* stream) {
+  if (!in || !grid || !out || coarsen <= 0 || nlabels < 0 || in->N != out->N || !scratch)
     return set_error(NZ_ERR_ARG, "nz_state_sort: bad arguments");
   BinGrid b;
   b.g = Grid{grid->Lx, grid->Ly, grid->Lz, grid->dLx, grid->dLy, grid->dLz, float(grid->nx), float(grid->ny),
@@ -209,8 +215,9 @@ extern "C" int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarse
   b.bx = (grid->nx + coarsen - 1) / coarsen;
   b.by = (grid->ny + coarsen - 1) / coarsen;
   b.bz = (grid->nz + coarsen - 1) / coarsen;
-  const long long nbins = 1ll * b.bx * b.by * b.bz;
-  if (nbins > (1 << 26)) return set_error(NZ_ERR_ARG, "nz_state_sort: %lld bins, coarsen more", nbins);
+  b.nlabels = nlabels;
+  const long long nbins = 1ll * b.bx * b.by * b.bz * (nlabels > 0 ? nlabels : 1);
+  if (nbins > (1 << 26)) return set_error(NZ_ERR_ARG, "nz_state_sort: %lld keys, coarsen more", nbins);
   const int N = in->N;
   const size_t need = nz_sort_scratch_bytes(N, int(nbins));
   if (scratch_bytes < need)
@@ -230,6 +237,11 @@ extern "C" int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarse
   if (rc) return rc;
   bin_scatter_kernel<<<(N + 255) / 256, 256, 0, st>>>(*in, N, bins, cursor, *out);
   return check_launch("bin_scatter_kernel");
+}
+
+extern "C" int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out, void* scratch,
+                             size_t scratch_bytes, void* stream) {
+  return nz_state_sort_keyed(in, grid, coarsen, 0, out, scratch, scratch_bytes, stream);
 }
 
 extern "C" int nz_signal_phi(const nz_state* st, const float* dirs, int ndir, const float* amp, int nb, double* out,

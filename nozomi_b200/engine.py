@@ -100,8 +100,9 @@ class DeviceSubstrate:
         self.n_items = n
         self.cell_sph4 = torch.empty((max(n, 1), 4), dtype=torch.float32, device=dev)
         self.cell_sid = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
-        L.check(L.load().nz_cells_gather(_p(self.spheres), self.S, _p(self.cell_items), n, _p(self.cell_sph4),
-                                         _p(self.cell_sid), _stream()), "nz_cells_gather")
+        L.check(L.load().nz_cells_gather(_p(self.spheres), self.S, _p(self.cell_items), n, _p(self.cell_start),
+                                         _p(self.cell_count), self.ncell, _p(self.cell_sph4), _p(self.cell_sid),
+                                         _stream()), "nz_cells_gather")
 
     def max_count(self) -> int:
         return int(self.cell_count.max().item()) if self.ncell else 0
@@ -244,14 +245,17 @@ class FusedState:
     def walker_ids(self) -> torch.Tensor:
         return self.org[:, 3].contiguous().view(torch.int32)
 
-    def sort_into(self, other: "FusedState", grid: L.Grid, coarsen: int, scratch: torch.Tensor | None = None):
-        nb = (-(-grid.nx // coarsen)) * (-(-grid.ny // coarsen)) * (-(-grid.nz // coarsen))
+    def sort_into(self, other: "FusedState", grid: L.Grid, coarsen: int, scratch: torch.Tensor | None = None,
+                  nlabels: int = 0):
+        """Re-bin into `other` by cell (coarsened), or by (label, cell) when
+        nlabels > 0.  Returns the scratch buffer for reuse."""
+        nb = (-(-grid.nx // coarsen)) * (-(-grid.ny // coarsen)) * (-(-grid.nz // coarsen)) * max(nlabels, 1)
         need = int(L.load().nz_sort_scratch_bytes(self.N, nb))
         if scratch is None or scratch.numel() < need:
             scratch = torch.empty(need, dtype=torch.uint8, device=_dev())
         a, b = self.struct(), other.struct()
-        L.check(L.load().nz_state_sort(L.byref(a), L.byref(grid), coarsen, L.byref(b), _p(scratch), scratch.numel(),
-                                       _stream()), "nz_state_sort")
+        L.check(L.load().nz_state_sort_keyed(L.byref(a), L.byref(grid), coarsen, int(nlabels), L.byref(b), _p(scratch),
+                                             scratch.numel(), _stream()), "nz_state_sort_keyed")
         return scratch
 
     def signal(self, dirs: torch.Tensor, amps: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:

@@ -26,7 +26,8 @@ class Tuning:
     """Launch shape of the fused walk (chosen by nozomi_b200.autotune)."""
     cell: float = 1.0             # cell edge, um
     steps_per_launch: int = 500   # steps between walker re-binnings
-    coarsen: int = 2              # re-binning bins = cells coarsened by this factor per axis
+    coarsen: int = 4              # re-binning bins = cells coarsened by this factor per axis
+    by_label: bool = True         # re-bin by (label, bin): a warp's walkers share a structure
 
 
 def device_substrate(sub: Substrate, D=2.0, T2=100.0, cell: float = 1.0, nseg=None, D_box=None,
@@ -68,28 +69,42 @@ class DwiRun:
         self._scratch = None
         self.launches = 0
 
-    def initial_positions(self) -> torch.Tensor:
+    def initial_positions(self):
+        """(positions [3,N], labels [N]) — given, or seeded on the device."""
         if self.positions is not None:
-            return self.positions
-        spins, _ = engine.seed(self.sub, self.targets, self.N, key=self.seed ^ 0x5EED)
-        return spins
+            return self.positions, None
+        return engine.seed(self.sub, self.targets, self.N, key=self.seed ^ 0x5EED)
 
-    def prepare(self, positions: torch.Tensor | None = None):
-        x = self.initial_positions() if positions is None else positions
+    def prepare(self, positions: torch.Tensor | None = None, labels: torch.Tensor | None = None):
+        if positions is None:
+            positions, labels = self.initial_positions()
+        x = positions
         N = x.shape[1]
-        wk = engine.Walkers(x, x.clone(), phi=torch.zeros((6, N), device=x.device))
+        lab = labels if labels is not None else torch.full((N,), -1, dtype=torch.int32, device=x.device)
+        wk = engine.Walkers(x, x.clone(), phi=torch.zeros((6, N), device=x.device), label=lab)
         self.state = engine.FusedState.from_walkers(wk)
         self.spare = engine.FusedState(N)
+        self.launches = 1
         return self
 
-    def walk(self):
+    def walk(self, events: list | None = None):
+        """All steps: re-bin, then one fused launch per steps_per_launch steps.
+        events: if a list, (start, end) CUDA events of each fused launch are
+        appended to it."""
         t = self.tuning
-        self.launches = 0
+        nl = self.sub.nstructures + 1 if t.by_label else 0
+        stream = torch.cuda.current_stream()
         for s0 in range(0, self.nsteps, t.steps_per_launch):
-            self._scratch = self.state.sort_into(self.spare, self.sub.grid, t.coarsen, self._scratch)
+            self._scratch = self.state.sort_into(self.spare, self.sub.grid, t.coarsen, self._scratch, nlabels=nl)
             self.state, self.spare = self.spare, self.state
+            if events is not None:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
             engine.walk_fused(self.sub, self.state, L.MODE_PHI, self.dt, self.G, self.Garea, s0,
                               min(self.nsteps, s0 + t.steps_per_launch), self.draws)
+            if events is not None:
+                e1.record(stream)
+                events.append((e0, e1))
             self.launches += 4
         return self
 

@@ -135,9 +135,11 @@ def test_fused_matches_oracle_and_reference(eng, name):
     np.testing.assert_allclose(wk.sig.cpu().numpy(), sig, rtol=2e-6)
 
 
-def test_fused_chunked_and_sorted_equals_single_launch(eng):
+@pytest.mark.parametrize("by_label", [False, True])
+def test_fused_chunked_and_sorted_equals_single_launch(eng, by_label):
     """Splitting the steps over launches and re-binning walkers between them
-    changes nothing: draws are keyed by walker id and step."""
+    (by cell, or by label and cell) changes nothing: draws are keyed by walker
+    id and step."""
     c = load("dwi_c1_cells")
     sub = _sub_from_case(eng, c, padded=False)
     N, nt, dt = int(c["N"]), int(c["nt"]), float(c["dt"])
@@ -154,8 +156,9 @@ def test_fused_chunked_and_sorted_equals_single_launch(eng):
     b = fresh()
     tmp = eng.FusedState(N)
     scratch = None
+    nl = int(c["nstructures"]) + 1 if by_label else 0
     for s0 in range(0, nt, 700):
-        scratch = b.sort_into(tmp, sub.grid, 2, scratch)
+        scratch = b.sort_into(tmp, sub.grid, 2, scratch, nlabels=nl)
         b, tmp = tmp, b
         eng.walk_fused(sub, b, eng.L.MODE_PHI, dt, G, Ga, s0, min(nt, s0 + 700), d)
     ia = a.walker_ids().cpu().numpy()
