@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--steps-per-launch", type=int, default=None)
     ap.add_argument("--coarsen", type=int, default=None)
     ap.add_argument("--by-label", type=int, default=None, help="re-bin by (label, bin): 1, or by bin only: 0")
+    ap.add_argument("--near-margin", type=float, default=None, help="near-list margin in um (0: none)")
     return ap.parse_args()
 
 
@@ -211,7 +212,9 @@ def run_ours(args):
         tuning.coarsen = args.coarsen
     if args.by_label is not None:
         tuning.by_label = bool(args.by_label)
-    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell)
+    if args.near_margin is not None:
+        tuning.near_margin = args.near_margin if args.near_margin > 0 else None
+    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin)
     amps = pg.amplitude_for_b(bvals)
     N = args.walkers
     run = DwiRun(dsub, pg, dirs, amps, N, seed=1000 + rank, tuning=tuning)
@@ -251,24 +254,44 @@ def run_ours(args):
         one_step()
         flush.zero_()
     barrier()
+    # one step captured as a CUDA graph (pack, re-bins, fused launches, signal)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        sig_static = one_step()
+    graph.replay()
+    barrier()
+
     clocks = Clocks(local)
     clocks.start()
-    step_ms, walk_ms, n_walk = 0.0, 0.0, 0
-    sig = None
+    step_ms = 0.0
     for _ in range(args.steps):
         flush.zero_()  # L2 flush between timed steps (outside the step's events)
         torch.cuda.synchronize()
-        ev = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        sig = one_step(ev)
+        graph.replay()
         e1.record(stream)
         torch.cuda.synchronize()
         step_ms += e0.elapsed_time(e1)
-        walk_ms += sum(a.elapsed_time(b) for a, b in ev)
-        n_walk += len(ev)
     barrier()
     clk = clocks.stop()
+    sig = sig_static.clone()
+
+    # the same step launched eagerly with CUDA events around every fused launch:
+    # the dominant kernel's average duration and its share of the step
+    walk_ms, n_walk = 0.0, 0
+    flush.zero_()
+    torch.cuda.synchronize()
+    ev = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    one_step(ev)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    eager_ms = e0.elapsed_time(e1)
+    walk_ms = sum(a.elapsed_time(b) for a, b in ev)
+    n_walk = len(ev)
+
     t_local = torch.tensor([step_ms, walk_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
@@ -278,17 +301,19 @@ def run_ours(args):
     S = sig.cpu().numpy()
     S = (S[0] + 1j * S[1]) / N
 
-    # end to end through the public call with host buffers
+    # end to end with host buffers: positions copied from pinned host memory
+    # into the graph's input, the step replayed, the signal copied back
     x_host = x0.cpu().pin_memory()
     e2e_ms = 0.0
     out_bytes = 0
+    host = torch.empty_like(sig_static, device="cpu").pin_memory()
     for i in range(args.e2e_steps + 1):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        xd = x_host.to("cuda", non_blocking=True)
-        sig_d = one_step(x=xd)
-        host = sig_d.to("cpu")
+        x0.copy_(x_host, non_blocking=True)
+        graph.replay()
+        host.copy_(sig_static, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize()
         out_bytes = host.numel() * host.element_size()
@@ -298,12 +323,13 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
     e2e_value = ws_per_step * args.e2e_steps / (float(t_local[0]) * 1e-3)
+    del graph
 
     line = None
     if rank == 0:
         walk_launch_ms = walk_ms / max(n_walk, 1)
         per_launch_ws = N * tuning.steps_per_launch
-        kernel_ws_s = N * run.nsteps * args.steps / (walk_ms * 1e-3)
+        kernel_ws_s = N * run.nsteps / (walk_ms * 1e-3)
         cpu = None
         wk = None
         if world == 1 and not args.no_cpu_baseline:
@@ -335,7 +361,9 @@ def run_ours(args):
                 "config": {"workload": WORKLOAD, "walkers_per_gpu": N, "time_steps": run.nsteps,
                            "directions": int(dirs.shape[1]), "bvalues": bvals.tolist(),
                            "cell_um": tuning.cell, "steps_per_launch": tuning.steps_per_launch,
-                           "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label, "spheres": sub.S, "cells": dsub.ncell,
+                           "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label, "near_margin_um": tuning.near_margin,
+                           "near_list_entries": int(dsub.near[2].numel()) if dsub.near is not None else 0,
+                           "spheres": sub.S, "cells": dsub.ncell,
                            "cell_list_entries": dsub.n_items, "l2": "256 MiB flush between timed steps",
                            "parallelism": f"walkers sharded over {world} GPU(s)"},
                 "e2e": {"value": e2e_value, "unit": "walker-steps/s",
@@ -344,7 +372,9 @@ def run_ours(args):
                 "gpu_launches": launches_per_step * args.steps,
                 "kernel": {"name": "walk_fused_kernel", "launches": n_walk, "avg_launch_ms": walk_launch_ms,
                            "walker_steps_per_launch": per_launch_ws, "kernel_walker_steps_per_s": kernel_ws_s,
-                           "share_of_step": walk_ms / step_ms},
+                           "share_of_step": walk_ms / eager_ms, "eager_step_ms": eager_ms,
+                           "timing": "value from CUDA-graph replays of the step; kernel figures from one eager "
+                                     "step with events around each fused launch"},
                 "roofline": roof_hbm, "roofline_fp32": roof_fp32, "cpu_baseline": cpu, "clocks": clk,
                 "signal_b0_mean": float(np.mean(np.abs(S[:, 0]))),
                 "signal_mean_by_b": [float(np.mean(S[:, b].real)) for b in range(S.shape[1])]}

@@ -68,6 +68,17 @@ typedef struct nz_substrate {
     const int* cell_sid;       /* [n_items] structure id of each list entry (fused walk) */
     const float* D;            /* [nstructures + 1] um^2/ms */
     const float* T2;           /* [nstructures + 1] ms */
+    /* Optional near lists on the same grid, built with a smaller margin
+     * near_margin (< the margin of the lists above): the fused walk scans them
+     * for an iteration whose walker-to-cell distance plus reach fits inside
+     * near_margin (then every sphere it can hit is in them and every sphere in
+     * them is in the full list, so the result is the full list's), the full
+     * lists otherwise.  near_sph4 == NULL: no near lists. */
+    float near_margin;
+    const int* near_start;
+    const int* near_count;
+    const float* near_sph4;
+    const int* near_sid;
 } nz_substrate;
 
 /* Source of the normal draws: an injected table normals[N][nsteps][maxk]

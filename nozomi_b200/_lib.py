@@ -31,7 +31,8 @@ class Grid(ctypes.Structure):
 class Substrate(ctypes.Structure):
     _fields_ = [("grid", Grid), ("nstructures", _i), ("S", _i), ("spheres", _P), ("cell_start", _P),
                 ("cell_count", _P), ("cell_items", _P), ("cell_sph4", _P), ("cell_sid", _P), ("D", _P),
-                ("T2", _P)]
+                ("T2", _P), ("near_margin", _f), ("near_start", _P), ("near_count", _P), ("near_sph4", _P),
+                ("near_sid", _P)]
 
 
 class Draws(ctypes.Structure):

@@ -139,6 +139,11 @@ static int check_fused_sub(const nz_substrate* sub, const char* who) {
   if (rc) return rc;
   if (!sub->cell_sph4 || !sub->cell_sid) return set_error(NZ_ERR_ARG, "%s: substrate lacks cell_sph4/cell_sid", who);
   if (!aligned16(sub->cell_sph4)) return set_error(NZ_ERR_ARG, "%s: cell_sph4 must be 16-byte aligned", who);
+  if (sub->near_sph4) {
+    if (!sub->near_start || !sub->near_count || !sub->near_sid || !(sub->near_margin > 0.0f))
+      return set_error(NZ_ERR_ARG, "%s: incomplete near lists", who);
+    if (!aligned16(sub->near_sph4)) return set_error(NZ_ERR_ARG, "%s: near_sph4 must be 16-byte aligned", who);
+  }
   return NZ_OK;
 }
 

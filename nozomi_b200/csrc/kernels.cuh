@@ -70,6 +70,12 @@ struct JobDev {
   float4* comp;
   double* moments;
   int nwalkers;
+  // near lists (null sph4: none)
+  float near_margin;
+  const int* near_start;
+  const int* near_count;
+  const float4* near_sph4;
+  const int* near_sid;
 };
 
 __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, const float* Garea, int nsteps, float dt,

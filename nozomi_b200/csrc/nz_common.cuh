@@ -159,11 +159,15 @@ struct Grid {
 
 // Cell of a position: clamped floor, idxSeg = iz*nx*ny + iy*nx + ix evaluated
 // in float as sim3d_kernel.cu:754-756 does.
-__device__ __forceinline__ int cell_of(const Grid& g, float x, float y, float z) {
-  const float fz = ref_min(g.nLz - 1, ref_max(0, floorf((z + g.Lz / 2) / g.dLz)));
-  const float fy = ref_min(g.nLy - 1, ref_max(0, floorf((y + g.Ly / 2) / g.dLy)));
-  const float fx = ref_min(g.nLx - 1, ref_max(0, floorf((x + g.Lx / 2) / g.dLx)));
+__device__ __forceinline__ int cell_of(const Grid& g, float x, float y, float z, float& fx, float& fy, float& fz) {
+  fz = ref_min(g.nLz - 1, ref_max(0, floorf((z + g.Lz / 2) / g.dLz)));
+  fy = ref_min(g.nLy - 1, ref_max(0, floorf((y + g.Ly / 2) / g.dLy)));
+  fx = ref_min(g.nLx - 1, ref_max(0, floorf((x + g.Lx / 2) / g.dLx)));
   return int(fz * g.nLx * g.nLy + fy * g.nLx + fx);
+}
+__device__ __forceinline__ int cell_of(const Grid& g, float x, float y, float z) {
+  float fx, fy, fz;
+  return cell_of(g, x, y, z, fx, fy, fz);
 }
 
 // ---------------------------------------------------------------------------

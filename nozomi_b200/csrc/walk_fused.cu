@@ -159,14 +159,18 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
   if (label < 0 || label > J.nstructures) label = J.nstructures;
 
   const float dt = J.dt;
+  const bool has_near = J.near_sph4 != nullptr;
   int s = s0;
-  int niter = 0, draw = 0, start = 0, count = 0;
+  int niter = 0, draw = 0, cell = 0;
+  float lox = 0.f, loy = 0.f, loz = 0.f;  // low corner of the step's cell
   float jr = 1.0f, ds = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
   while (s < s1) {
     if (niter == 0) {
-      const int cell = cell_of(J.g, x, y, z);
-      start = __ldg(J.cell_start + cell);
-      count = __ldg(J.cell_count + cell);
+      float cx, cy, cz;
+      cell = cell_of(J.g, x, y, z, cx, cy, cz);
+      lox = cx * J.g.dLx - J.g.Lx / 2;
+      loy = cy * J.g.dLy - J.g.Ly / 2;
+      loz = cz * J.g.dLz - J.g.Lz / 2;
       jr = 1.0f;
       draw = 0;
     }
@@ -178,15 +182,34 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
       draw = 1;
     }
     float a = jx * jx + jy * jy + jz * jz;
+    float reach = sqrtf(a) * jr;
+    // Near list when everything this iteration can touch lies within its
+    // margin of the step's cell: distance from the walker to the cell plus
+    // the reach, with 2 % + 2 nm of slack against rounding.
+    bool near = false;
+    if (has_near) {
+      const float ex = fmaxf(0.f, fmaxf(lox - x, x - (lox + J.g.dLx)));
+      const float ey = fmaxf(0.f, fmaxf(loy - y, y - (loy + J.g.dLy)));
+      const float ez = fmaxf(0.f, fmaxf(loz - z, z - (loz + J.g.dLz)));
+      const float dist = sqrtf(ex * ex + ey * ey + ez * ez);
+      near = (dist + reach) * 1.02f + kTol + 2e-3f <= J.near_margin;
+    }
+    const float4* sph4 = near ? J.near_sph4 : J.sph4;
+    const int* sidv = near ? J.near_sid : J.sid;
+    const int start = __ldg((near ? J.near_start : J.cell_start) + cell);
+    const int count = __ldg((near ? J.near_count : J.cell_count) + cell);
     ScanOut r;
-    if (!scan_cell(J.sph4, J.sid, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, sqrtf(a) * jr, r)) {
-      label = label_of(J.sph4, J.sid, start, count, J.nstructures, x, y, z);
+    if (!scan_cell(sph4, sidv, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r)) {
+      label = label_of(sph4, sidv, start, count, J.nstructures, x, y, z);
       if (niter == 1) {  // the first draw's length depends on the label
         ds = sqrtf(2 * __ldg(J.D + label) * dt);
         jump_of(J, wid, s, 0, ds, jx, jy, jz);
         a = jx * jx + jy * jy + jz * jz;
+        reach = sqrtf(a) * jr;
       }
-      scan_cell(J.sph4, J.sid, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, sqrtf(a) * jr, r);
+      // the full list: the near one was chosen for the old reach
+      const int fs = __ldg(J.cell_start + cell), fc = __ldg(J.cell_count + cell);
+      scan_cell(J.sph4, J.sid, fs, fc, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r);
     }
     jc = ref_min(jc, r.any_in ? r.fin : kBig);
     jc = ref_min(jc, r.fout);
@@ -379,6 +402,11 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
   j.sid = sub.cell_sid;
   j.cell_start = sub.cell_start;
   j.cell_count = sub.cell_count;
+  j.near_margin = sub.near_margin;
+  j.near_start = sub.near_start;
+  j.near_count = sub.near_count;
+  j.near_sph4 = reinterpret_cast<const float4*>(sub.near_sph4);
+  j.near_sid = sub.near_sid;
   j.D = sub.D;
   j.T2 = sub.T2;
   j.G = G;

@@ -48,7 +48,7 @@ class DeviceSubstrate:
     per-entry sphere records of the fused walk, and D / T2 per structure."""
 
     def __init__(self, spheres: np.ndarray, nstructures: int, L3, nseg, D, T2, jump_tol: float = 1.0,
-                 cells: tuple | None = None):
+                 cells: tuple | None = None, near_margin: float | None = None):
         require_cuda()
         dev = _dev()
         sph64 = np.ascontiguousarray(spheres, dtype=np.float64).reshape(5, -1)
@@ -73,14 +73,19 @@ class DeviceSubstrate:
             self.cell_count = torch.as_tensor(np.asarray(ct, np.int32), device=dev)
             self.cell_items = torch.as_tensor(np.asarray(it, np.int32), device=dev)
         self._gather()
+        self.near_margin = None
+        self.near = None
+        if near_margin is not None:
+            self.set_near_margin(near_margin)
 
-    def _build_cells(self):
+    def _build_cells(self, margin: float | None = None, store: bool = True):
         dev = _dev()
         lib = L.load()
         Lx, Ly, Lz = self.L
         nx, ny, nz = self.nseg
+        tol = self.jump_tol if margin is None else float(margin)
         counts = torch.empty(self.ncell, dtype=torch.int32, device=dev)
-        L.check(lib.nz_cells_count(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, self.jump_tol, _p(counts),
+        L.check(lib.nz_cells_count(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, tol, _p(counts),
                                    _stream()), "nz_cells_count")
         offsets = torch.empty(self.ncell, dtype=torch.int32, device=dev)
         total = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -89,10 +94,31 @@ class DeviceSubstrate:
         n_items = int(total.item())  # one host sync: the list length sizes the item array
         items = torch.empty(max(n_items, 1), dtype=torch.int32, device=dev)
         cursor = torch.empty(self.ncell, dtype=torch.int32, device=dev)
-        L.check(lib.nz_cells_fill(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, self.jump_tol, _p(offsets),
+        L.check(lib.nz_cells_fill(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, tol, _p(offsets),
                                   _p(counts), _p(cursor), _p(items), _stream()), "nz_cells_fill")
+        if not store:
+            return offsets, counts, items
         self.cell_start, self.cell_count, self.cell_items = offsets, counts, items
         self.n_items = n_items
+
+    def set_near_margin(self, margin: float | None):
+        """Build (or drop, with None) the near lists of the fused walk: the
+        same grid with a smaller membership margin (0 < margin < jump_tol)."""
+        if margin is None:
+            self.near_margin, self.near = None, None
+            return
+        margin = float(margin)
+        if not 0.0 < margin < self.jump_tol:
+            raise NozomiError(f"near margin {margin} must lie in (0, {self.jump_tol})")
+        st, ct, it = self._build_cells(margin, store=False)
+        n = int(it.numel())
+        dev = _dev()
+        sph4 = torch.empty((max(n, 1), 4), dtype=torch.float32, device=dev)
+        sid = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+        L.check(L.load().nz_cells_gather(_p(self.spheres), self.S, _p(it), n, _p(st), _p(ct), self.ncell, _p(sph4),
+                                         _p(sid), _stream()), "nz_cells_gather")
+        self.near_margin = margin
+        self.near = (st, ct, it, sph4, sid)
 
     def _gather(self):
         dev = _dev()
@@ -128,16 +154,23 @@ class DeviceSubstrate:
         other.cell_items = seg
         other._gather()
         other.K = K
+        other.near_margin, other.near = None, None
         return other
 
     def struct(self) -> L.Substrate:
-        return L.Substrate(self.grid, self.nstructures, self.S, self.spheres.data_ptr(), self.cell_start.data_ptr(),
-                           self.cell_count.data_ptr(), self.cell_items.data_ptr(), self.cell_sph4.data_ptr(),
-                           self.cell_sid.data_ptr(), self.D.data_ptr(), self.T2.data_ptr())
+        s = L.Substrate(self.grid, self.nstructures, self.S, self.spheres.data_ptr(), self.cell_start.data_ptr(),
+                        self.cell_count.data_ptr(), self.cell_items.data_ptr(), self.cell_sph4.data_ptr(),
+                        self.cell_sid.data_ptr(), self.D.data_ptr(), self.T2.data_ptr())
+        if self.near is not None:
+            st, ct, _, sph4, sid = self.near
+            s.near_margin = self.near_margin
+            s.near_start, s.near_count = st.data_ptr(), ct.data_ptr()
+            s.near_sph4, s.near_sid = sph4.data_ptr(), sid.data_ptr()
+        return s
 
     def nbytes(self) -> int:
         ts = [self.spheres64, self.spheres, self.D, self.T2, self.cell_start, self.cell_count, self.cell_items,
-              self.cell_sph4, self.cell_sid]
+              self.cell_sph4, self.cell_sid] + (list(self.near) if self.near is not None else [])
         return sum(t.numel() * t.element_size() for t in ts)
 
 

@@ -28,17 +28,18 @@ class Tuning:
     steps_per_launch: int = 500   # steps between walker re-binnings
     coarsen: int = 4              # re-binning bins = cells coarsened by this factor per axis
     by_label: bool = True         # re-bin by (label, bin): a warp's walkers share a structure
+    near_margin: float | None = 0.5  # margin of the near lists (None: full lists only)
 
 
 def device_substrate(sub: Substrate, D=2.0, T2=100.0, cell: float = 1.0, nseg=None, D_box=None,
-                     jump_tol: float = 1.0) -> engine.DeviceSubstrate:
+                     jump_tol: float = 1.0, near_margin: float | None = None) -> engine.DeviceSubstrate:
     nseg = cell_grid(sub.L, cell) if nseg is None else nseg
     ns = sub.nstructures
     Dv = np.full(ns + 1, D, np.float32)
     if D_box is not None:
         Dv[ns] = D_box
     T2v = np.full(ns + 1, T2, np.float32)
-    return engine.DeviceSubstrate(sub.spheres(), ns, sub.L, nseg, Dv, T2v, jump_tol=jump_tol)
+    return engine.DeviceSubstrate(sub.spheres(), ns, sub.L, nseg, Dv, T2v, jump_tol=jump_tol, near_margin=near_margin)
 
 
 class DwiRun:
@@ -132,6 +133,6 @@ def simulate_dwi(sub: Substrate, gwave, dirs, bvalues=None, amplitudes=None, N: 
     if amplitudes is None:
         amplitudes = gwave.amplitude_for_b(bvalues)
     tuning = tuning or Tuning()
-    dsub = device_substrate(sub, D=D, T2=T2, cell=tuning.cell)
+    dsub = device_substrate(sub, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin)
     run = DwiRun(dsub, gwave, dirs, amplitudes, N, seed=seed, targets=targets, tuning=tuning).prepare()
     return run.walk().signal()

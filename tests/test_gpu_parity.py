@@ -257,3 +257,38 @@ def test_signal_and_moments_match_oracle(eng):
     m = torch.zeros(6, dtype=torch.float64, device="cuda")
     eng.moments(x, _dev(s0), m)
     np.testing.assert_allclose(m.cpu().numpy(), oz.moments(x.cpu().numpy(), s0), rtol=1e-10)
+
+
+@pytest.mark.parametrize("name,margin", [("dwi_c1_cells", 0.5), ("dwi_c1_cells", 0.25), ("dwi_overlap", 0.4),
+                                         ("narrow_periodic_in", 0.3)])
+def test_fused_near_lists_match_full_lists(eng, name, margin):
+    """Near lists (smaller margin, used when an iteration's reach fits) give
+    the full lists' result bit for bit: the fused walk with near lists against
+    the oracle on the full member lists."""
+    c = load(name)
+    sph, L3, nseg = c["spheres"], tuple(c["L"]), tuple(int(v) for v in c["nseg"])
+    sub = eng.DeviceSubstrate(sph, int(c["nstructures"]), L3, nseg, c["D"], c["T2"], near_margin=margin)
+    assert sub.near is not None and sub.near[2].numel() < sub.n_items
+    st_, ct, it = cells_members(sph, L3, nseg)
+    g = oz.Geometry(sph.astype(np.float32), int(c["nstructures"]), L3, nseg, st_, ct, it, c["D"], c["T2"],
+                    dL=tuple(c["dL"]))
+    N, nt, dt = int(c["N"]), int(c["nt"]), float(c["dt"])
+    G = c["G"] if "G" in c else np.zeros(nt, np.float32)
+    Ga = c["Garea"] if "Garea" in c else np.zeros(nt, np.float32)
+    x0 = c["x0"].astype(np.float32)
+    spins, spins0 = x0.copy(), x0.copy()
+    phi = np.zeros((6, N), np.float32)
+    r = oz.walk_f32(g, oz.philox(17), oz.MODE_PHI, spins, spins0, 0, nt, dt, G=G, Garea=Ga, phi=phi)
+    x = _dev(x0)
+    wk = eng.Walkers(x, x.clone(), phi=torch.zeros((6, N), device="cuda"),
+                     label=torch.full((N,), -1, dtype=torch.int32, device="cuda"),
+                     flags=torch.zeros(N, dtype=torch.int32, device="cuda"))
+    st = eng.FusedState.from_walkers(wk)
+    eng.walk_fused(sub, st, eng.L.MODE_PHI, dt, _dev(G.astype(np.float32)), _dev(Ga.astype(np.float32)), 0, nt,
+                   eng.philox_draws(17))
+    st.to_walkers(wk)
+    np.testing.assert_array_equal(wk.spins.cpu().numpy(), spins)
+    np.testing.assert_array_equal(wk.spins0.cpu().numpy(), spins0)
+    np.testing.assert_array_equal(wk.phi.cpu().numpy(), phi)
+    np.testing.assert_array_equal(wk.label.cpu().numpy(), r["label"])
+    np.testing.assert_array_equal(wk.flags.cpu().numpy(), r["flags"])
