@@ -195,6 +195,10 @@ int nz_walk_step(const nz_substrate* sub, const nz_walkers* wk, int mode, float 
  * loop, diffsim3d.py:246-261, moved onto the device). ---- */
 int nz_state_pack(const nz_walkers* wk, const uint32_t* walker_id, nz_state* st, void* stream);
 int nz_state_unpack(const nz_state* st, const nz_walkers* wk, void* stream);
+/* Unpack in walker-id order: the walker whose id is i goes to column i of the
+ * reference layout, undoing any re-binning (ids must be 0..N-1; others are
+ * dropped and counted in *n_bad, a device int, when n_bad is not NULL). */
+int nz_state_unpack_by_id(const nz_state* st, const nz_walkers* wk, int* n_bad, void* stream);
 
 int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mode, float dt, const float* G,
                   const float* Garea, int step0, int step1, const nz_draws* draws, double* moments,

@@ -130,7 +130,17 @@ extern "C" int nz_state_unpack(const nz_state* st, const nz_walkers* wk, void* s
   if (rc) return rc;
   if (!wk || wk->N != st->N || !wk->spins || !wk->spins0) return set_error(NZ_ERR_ARG, "nz_state_unpack: bad walkers");
   if (st->N == 0) return NZ_OK;
-  unpack_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*st, *wk);
+  unpack_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*st, *wk, 0, nullptr);
+  return check_launch("unpack_kernel");
+}
+
+extern "C" int nz_state_unpack_by_id(const nz_state* st, const nz_walkers* wk, int* n_bad, void* stream) {
+  int rc = check_state(st, "nz_state_unpack_by_id");
+  if (rc) return rc;
+  if (!wk || wk->N != st->N || !wk->spins || !wk->spins0)
+    return set_error(NZ_ERR_ARG, "nz_state_unpack_by_id: bad walkers");
+  if (st->N == 0) return NZ_OK;
+  unpack_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*st, *wk, 1, n_bad);
   return check_launch("unpack_kernel");
 }
 

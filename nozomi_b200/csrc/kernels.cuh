@@ -83,7 +83,7 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
 int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
                  int step1, int* queue, int grid, cudaStream_t st);
 __global__ void pack_kernel(nz_walkers wk, const uint32_t* ids, nz_state st);
-__global__ void unpack_kernel(nz_state st, nz_walkers wk);
+__global__ void unpack_kernel(nz_state st, nz_walkers wk, int by_id, int* bad);
 
 // ---- cells.cu ----
 __global__ void scan_kernel(const int* __restrict__ in, int* __restrict__ out, int n, int* __restrict__ total);

@@ -372,14 +372,24 @@ __global__ void pack_kernel(nz_walkers wk, const uint32_t* __restrict__ ids, nz_
   reinterpret_cast<float4*>(st.comp)[w] = c;
 }
 
-__global__ void unpack_kernel(nz_state st, nz_walkers wk) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= wk.N) return;
+// by_id: walker w of the state goes to the reference-layout slot of its
+// walker id (ids outside [0, N) are dropped and counted in *bad).
+__global__ void unpack_kernel(nz_state st, nz_walkers wk, int by_id, int* bad) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= wk.N) return;
+  int w = slot;
+  if (by_id) {
+    w = __float_as_int(reinterpret_cast<const float4*>(st.org)[slot].w);
+    if (w < 0 || w >= wk.N) {
+      if (bad) atomicAdd(bad, 1);
+      return;
+    }
+  }
   const int N = wk.N;
-  const float4 p = reinterpret_cast<const float4*>(st.pos)[w];
-  const float4 o = reinterpret_cast<const float4*>(st.org)[w];
-  const float4 f = reinterpret_cast<const float4*>(st.phi)[w];
-  const float4 c = reinterpret_cast<const float4*>(st.comp)[w];
+  const float4 p = reinterpret_cast<const float4*>(st.pos)[slot];
+  const float4 o = reinterpret_cast<const float4*>(st.org)[slot];
+  const float4 f = reinterpret_cast<const float4*>(st.phi)[slot];
+  const float4 c = reinterpret_cast<const float4*>(st.comp)[slot];
   wk.spins[w] = p.x; wk.spins[N + w] = p.y; wk.spins[2 * N + w] = p.z;
   wk.spins0[w] = o.x; wk.spins0[N + w] = o.y; wk.spins0[2 * N + w] = o.z;
   if (wk.label) wk.label[w] = __float_as_int(p.w);

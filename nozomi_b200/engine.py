@@ -72,6 +72,7 @@ class DeviceSubstrate:
             self.cell_start = torch.as_tensor(np.asarray(st, np.int32), device=dev)
             self.cell_count = torch.as_tensor(np.asarray(ct, np.int32), device=dev)
             self.cell_items = torch.as_tensor(np.asarray(it, np.int32), device=dev)
+            self.n_items = int(self.cell_items.numel())
         self._gather()
         self.near_margin = None
         self.near = None
@@ -97,7 +98,7 @@ class DeviceSubstrate:
         L.check(lib.nz_cells_fill(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, tol, _p(offsets),
                                   _p(counts), _p(cursor), _p(items), _stream()), "nz_cells_fill")
         if not store:
-            return offsets, counts, items
+            return offsets, counts, items, n_items
         self.cell_start, self.cell_count, self.cell_items = offsets, counts, items
         self.n_items = n_items
 
@@ -110,8 +111,7 @@ class DeviceSubstrate:
         margin = float(margin)
         if not 0.0 < margin < self.jump_tol:
             raise NozomiError(f"near margin {margin} must lie in (0, {self.jump_tol})")
-        st, ct, it = self._build_cells(margin, store=False)
-        n = int(it.numel())
+        st, ct, it, n = self._build_cells(margin, store=False)
         dev = _dev()
         sph4 = torch.empty((max(n, 1), 4), dtype=torch.float32, device=dev)
         sid = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
@@ -122,8 +122,7 @@ class DeviceSubstrate:
 
     def _gather(self):
         dev = _dev()
-        n = int(self.cell_items.numel())
-        self.n_items = n
+        n = int(self.n_items)
         self.cell_sph4 = torch.empty((max(n, 1), 4), dtype=torch.float32, device=dev)
         self.cell_sid = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
         L.check(L.load().nz_cells_gather(_p(self.spheres), self.S, _p(self.cell_items), n, _p(self.cell_start),
@@ -152,6 +151,7 @@ class DeviceSubstrate:
         other.cell_start = torch.arange(self.ncell, dtype=torch.int32, device=dev) * K
         other.cell_count = torch.full((self.ncell,), K, dtype=torch.int32, device=dev)
         other.cell_items = seg
+        other.n_items = int(seg.numel())
         other._gather()
         other.K = K
         other.near_margin, other.near = None, None
@@ -274,6 +274,14 @@ class FusedState:
         s = self.struct()
         w = wk.struct()
         L.check(L.load().nz_state_unpack(L.byref(s), L.byref(w), _stream()), "nz_state_unpack")
+
+    def to_walkers_by_id(self, wk: Walkers):
+        """Unpack into walker-id order (undoes re-binning)."""
+        s = self.struct()
+        w = wk.struct()
+        bad = torch.zeros(1, dtype=torch.int32, device=_dev())
+        L.check(L.load().nz_state_unpack_by_id(L.byref(s), L.byref(w), _p(bad), _stream()), "nz_state_unpack_by_id")
+        return bad
 
     def walker_ids(self) -> torch.Tensor:
         return self.org[:, 3].contiguous().view(torch.int32)

@@ -119,10 +119,22 @@ class DwiRun:
         s = self.signal_sums().cpu().numpy()
         return (s[0] + 1j * s[1]) / self.state.N
 
+    def walkers(self) -> engine.Walkers:
+        """The walkers in walker-id order, reference layout (positions, spins0,
+        Phi [6,N], label, flags)."""
+        N = self.state.N
+        dev = self.state.pos.device
+        wk = engine.Walkers(torch.empty((3, N), device=dev), torch.empty((3, N), device=dev),
+                            phi=torch.empty((6, N), device=dev), label=torch.empty(N, dtype=torch.int32, device=dev),
+                            flags=torch.empty(N, dtype=torch.int32, device=dev))
+        self.state.to_walkers_by_id(wk)
+        return wk
+
     def phase(self) -> torch.Tensor:
         """Per-walker phase [ndir, N] of the unit waveform, walker-id order."""
-        order = torch.argsort(self.state.walker_ids())
-        return self.state.phase(self.dirs)[:, order]
+        wk = self.walkers()
+        st = engine.FusedState.from_walkers(wk)
+        return st.phase(self.dirs)
 
 
 def simulate_dwi(sub: Substrate, gwave, dirs, bvalues=None, amplitudes=None, N: int = 100000, D=2.0, T2=100.0,

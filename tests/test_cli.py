@@ -1,0 +1,70 @@
+"""CLI and configuration (host logic on CPU; one end-to-end run on the GPU)."""
+import json
+import pickle
+
+import numpy as np
+import pytest
+
+from nozomi_b200 import config as cfg
+from nozomi_b200.cli.main import parser, substrate_files
+from nozomi_b200 import substrates as sb
+
+
+def test_config_merge_keeps_file_values_for_unset_args():
+    c = cfg.load_config_file(cfg.SIM_CONFIG_FILE)
+    m = cfg.merge(c, {"nseg": None, "sim_time": 5.0})
+    assert m["nseg"] == c["nseg"] and m["sim_time"] == 5.0
+
+
+def test_parser_subcommands():
+    a = parser().parse_args(["simulation", "--substrates", "x", "--sim_time", "2", "--nseg", "3"])
+    assert a.command == "simulation" and a.sim_time == 2.0 and a.nseg == 3
+    g = parser().parse_args(["gradient_simulation", "--substrates", "x"])
+    assert g.config.endswith("pgse_sim_params.json")
+
+
+def _write_substrate(tmp_path):
+    """Two straight fibres in the reference's pickle format (last sphere of a
+    fibre at z == L/2)."""
+    L = 10.0
+    rows = []
+    for fid, (x, y) in enumerate([(-2.0, 0.0), (2.5, 1.0)]):
+        for z in np.linspace(-L / 2 + 0.3, L / 2, 30):
+            rows.append([x, y, z, 1.0, fid])
+    d = tmp_path / "exp" / "run1" / "data"
+    d.mkdir(parents=True)
+    sb.save_pickle(d / "sub.pkl", np.array(rows), L)
+    return tmp_path / "exp", L
+
+
+def test_substrate_walk_and_ingestion(tmp_path):
+    root, L = _write_substrate(tmp_path)
+    files = substrate_files(str(root))
+    assert len(files) == 1
+    s = sb.from_pickle(files[0])
+    assert s.nstructures == 2
+    assert all(f.shape[0] == 30 + 50 for f in s.fibers)  # z pads of 25 + 25 spheres
+
+
+@pytest.mark.gpu
+def test_cli_end_to_end(tmp_path):
+    from nozomi_b200.cli.main import main
+    root, L = _write_substrate(tmp_path)
+    conf = tmp_path / "sim.json"
+    conf.write_text(json.dumps({"time_step": 0.002, "num_spins": 20000, "D0_intra": 2.0, "D0_extra": 2.0,
+                                "nseg": 2, "sim_time": 1.0}))
+    assert main(["simulation", "--substrates", str(root), "--config", str(conf), "--compartment", "intra"]) == 0
+    out = list((root / "run1" / "sim" / "ADCdata").glob("diffcoeff_intra_*spins_sub_*.pkl"))
+    data = pickle.load(open([p for p in out if "kurtosis" not in p.name][0], "rb"))
+    assert data.shape == (500, 4)
+    # fibres along z: free along z, restricted across
+    assert 1.6 < data[-1, 2] < 2.4 and data[-1, 0] < 1.0
+    g = tmp_path / "g.json"
+    g.write_text(json.dumps({"time_step": 0.01, "num_spins": 5000, "D0_intra": 2.0, "D0_extra": 2.0, "nseg": 2,
+                             "sim_time": 30.0, "gradient": {"type": "PGSE", "direction": [[1, 0, 0], [0, 0, 1]],
+                                                            "big_delta": 20.0, "little_delta": 10.0}}))
+    assert main(["gradient_simulation", "--substrates", str(root), "--config", str(g)]) == 0
+    res = pickle.load(open(next((root / "run1" / "sim" / "DWIdata").glob("*.pkl")), "rb"))
+    assert res["phase"].shape == (2, 5000)
+    S = res["signal"].real
+    assert S[0, 0] == pytest.approx(1.0) and S[1, -1] < S[0, -1]  # along the fibres attenuates more
