@@ -53,6 +53,12 @@ def parse():
     ap.add_argument("--coarsen", type=int, default=None)
     ap.add_argument("--by-label", type=int, default=None, help="re-bin by (label, bin): 1, or by bin only: 0")
     ap.add_argument("--near-margin", type=float, default=None, help="near-list margin in um (0: none)")
+    ap.add_argument("--workload", default="packed", choices=["packed", "batched"],
+                    help="packed: one packed substrate (default); batched: 64 mixed substrates, batched vs plain")
+    ap.add_argument("--jobs", type=int, default=64, help="batched: number of substrates")
+    ap.add_argument("--walker-scale", type=float, default=1.0, help="batched: scale of the walker counts")
+    ap.add_argument("--threads", type=int, default=128, help="batched: walkers per CTA")
+    ap.add_argument("--plain-every", type=int, default=1, help="batched: time the plain path on every k-th job")
     return ap.parse_args()
 
 
@@ -385,10 +391,93 @@ def run_ours(args):
     return 0
 
 
+BATCH_WORKLOAD = ("batched mixed workload: {jobs} substrates of 10-500 beaded axons (40 spheres at 1 um, radii "
+                  "U[0.5,1.5], z-periodic, packed at area fraction 0.35), walkers log-uniform 1e4-1e6 (x{scale}), "
+                  "2000-8000 steps at dt=5 us (PGSE delta=te/3, Delta=2te/3), 6-60 directions, b={{0,1,2,3}} "
+                  "ms/um^2, seed 4")
+
+
+def run_batched(args):
+    import torch
+    from nozomi_b200 import engine
+    from nozomi_b200.batch import BatchRun, SubstrateCache
+    from nozomi_b200.plain import run_plain
+    from nozomi_b200.simulate import Tuning
+    from nozomi_b200.workloads import mixed_specs
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    engine.require_cuda()
+    specs = mixed_specs(seed=4, n_jobs=args.jobs, walker_scale=args.walker_scale)
+    tuning = Tuning()
+    if args.steps_per_launch:
+        tuning.steps_per_launch = args.steps_per_launch
+    if args.near_margin is not None:
+        tuning.near_margin = args.near_margin if args.near_margin > 0 else None
+    cache = SubstrateCache()
+    run = BatchRun(specs, tuning=tuning, threads=args.threads, cache=cache)
+    stream = torch.cuda.current_stream()
+    run.step()
+    for _ in range(max(0, args.warmup - 1)):
+        run.step()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        run.step()
+    torch.cuda.synchronize()
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    ms = 0.0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        graph.replay()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ws = run.walker_steps()
+    value = ws * args.steps / (ms * 1e-3)
+    sig_batched = run.signals()
+    # the plain per-substrate path, one job after another, launched from the host
+    sel = list(range(0, len(specs), args.plain_every))
+    plain_ms, plain_ws, err = 0.0, 0, 0.0
+    for i in sel:
+        sp = specs[i]
+        dsub = cache.get(sp.key, sp.substrate, sp.D, sp.T2, tuning)
+        x = run.positions[i][0]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = run_plain(dsub, sp, x)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        plain_ws += sp.N * sp.nsteps
+        o = out.cpu().numpy()
+        err = max(err, float(np.abs((o[0] + 1j * o[1]) / sp.N - sig_batched[i]).max()))
+    plain_value = plain_ws / (plain_ms * 1e-3)
+    line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded substrates, protocols and walkers)",
+            "config": {"workload": BATCH_WORKLOAD.format(jobs=len(specs), scale=args.walker_scale),
+                       "jobs": len(specs), "walker_steps_per_step": ws, "threads": args.threads,
+                       "steps_per_launch": tuning.steps_per_launch, "near_margin_um": tuning.near_margin,
+                       "persistent_grid": run.grid, "chunks": len(run.chunks)},
+            "gpu_launches": run.launches() * args.steps,
+            "plain": {"value": plain_value, "unit": "walker-steps/s", "jobs_timed": len(sel),
+                      "walker_steps_timed": plain_ws, "launch": "one plain-kernel launch per step from the host, "
+                      "per-direction phase in HBM, substrates one after another"},
+            "speedup_vs_plain": value / plain_value,
+            "max_signal_diff_batched_vs_plain": err, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
     return run_ours(args)
 
 

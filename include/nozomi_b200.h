@@ -208,9 +208,15 @@ int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mode, float d
  * of each job (clamped to its nsteps), CTAs pulling items from *queue (one
  * device int, zeroed by the caller) until none is left.  jobs and items are
  * device arrays; every job of one launch has mode `mode`.  grid = CTA count
- * (0 = one CTA per item, no queue).  Items hold at most 128 walkers. ---- */
+ * (0 = one CTA per item, no queue); threads = walkers per CTA (a multiple of
+ * 32 up to 256); an item holds at most `threads` walkers.  The batched form of
+ * the fused walk: many substrates, protocols and walker sets in one launch. */
 int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0, int step1,
-                  int* queue, int grid, void* stream);
+                  int* queue, int grid, int threads, void* stream);
+
+/* CTAs of `threads` walkers of the batched walk in `mode` that fit on one SM
+ * (the persistent grid is this times the SM count). */
+int nz_batch_occupancy(int mode, int threads, int* blocks_per_sm);
 
 /* ---- walker re-binning: a stable-key counting sort of the packed state by
  * cell, so that the walkers of one CTA share cells.  bins: bin per walker is
@@ -244,6 +250,10 @@ int nz_state_sort_static(const nz_state* in, const nz_grid* grid, int coarsen, n
  * (real then imaginary), accumulated into (zero it first). ---- */
 int nz_signal_phi(const nz_state* st, const float* dirs, int ndir, const float* amp, int nb, double* out,
                   void* stream);
+
+/* Signal from a per-direction phase array (the reference's phase_d layout,
+ * [ndir, N] float): out[2][ndir][nb] += sums of cos / sin(amp[b] * phase). */
+int nz_signal_phase(const float* phase, int ndir, int N, const float* amp, int nb, double* out, void* stream);
 
 /* Per-direction phase from Phi: phase[d][w] = u_d . (Phi_w - comp_w), float. */
 int nz_phase_from_phi(const nz_state* st, const float* dirs, int ndir, float* phase, void* stream);

@@ -74,7 +74,8 @@ SIGNATURES = {
     "nz_state_unpack": (_i, [_P, _P, _P]),
     "nz_state_unpack_by_id": (_i, [_P, _P, _P, _P]),
     "nz_walk_fused": (_i, [_P, _P, _i, _f, _P, _P, _i, _i, _P, _P, _P]),
-    "nz_walk_batch": (_i, [_P, _i, _P, _i, _i, _i, _i, _P, _i, _P]),
+    "nz_walk_batch": (_i, [_P, _i, _P, _i, _i, _i, _i, _P, _i, _i, _P]),
+    "nz_batch_occupancy": (_i, [_i, _i, _P]),
     "nz_sort_scratch_bytes": (ctypes.c_size_t, [_i, _i]),
     "nz_state_sort": (_i, [_P, _P, _i, _P, _P, ctypes.c_size_t, _P]),
     "nz_state_sort_keyed": (_i, [_P, _P, _i, _i, _P, _P, ctypes.c_size_t, _P]),
@@ -82,6 +83,7 @@ SIGNATURES = {
     "nz_state_sort_static": (_i, [_P, _P, _i, _P, _P]),
     "nz_signal_phi": (_i, [_P, _P, _i, _P, _i, _P, _P]),
     "nz_phase_from_phi": (_i, [_P, _P, _i, _P, _P]),
+    "nz_signal_phase": (_i, [_P, _i, _i, _P, _i, _P, _P]),
     "nz_moments": (_i, [_P, _P, _i, _P, _P]),
     "nz_probe_fma": (_i, [_i, _i, _P, _P]),
 }

@@ -176,18 +176,27 @@ extern "C" int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mo
   if (st->N == 0 || step1 == step0) return NZ_OK;
   const JobDev j = make_job(*sub, G, Garea, step1, dt, *draws, mode, *st, moments);
   const int n_items = (st->N + kFusedThreads - 1) / kFusedThreads;
-  return launch_fused(mode, j, nullptr, nullptr, n_items, step0, step1, nullptr, n_items,
+  return launch_fused(mode, j, nullptr, nullptr, n_items, step0, step1, nullptr, n_items, kFusedThreads,
                       static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0,
-                             int step1, int* queue, int grid, void* stream) {
+                             int step1, int* queue, int grid, int threads, void* stream) {
   if (!jobs || n_jobs <= 0 || !items || n_items < 0 || step0 < 0 || step1 < step0 || grid < 0)
     return set_error(NZ_ERR_ARG, "nz_walk_batch: bad arguments");
+  if (threads < 32 || threads > kFusedMaxThreads || threads % 32)
+    return set_error(NZ_ERR_ARG, "nz_walk_batch: threads %d not a multiple of 32 in [32, %d]", threads,
+                     kFusedMaxThreads);
   if (grid > 0 && !queue) return set_error(NZ_ERR_ARG, "nz_walk_batch: a persistent grid needs a queue counter");
   if (mode & NZ_MODE_MOMENTS) return set_error(NZ_ERR_ARG, "nz_walk_batch: moments are per-substrate (nz_walk_fused)");
   if (n_items == 0 || step1 == step0) return NZ_OK;
   const JobDev unused{};
   return launch_fused(mode, unused, jobs, items, n_items, step0, step1, grid > 0 ? queue : nullptr,
-                      grid > 0 ? grid : n_items, static_cast<cudaStream_t>(stream));
+                      grid > 0 ? grid : n_items, threads, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int nz_batch_occupancy(int mode, int threads, int* blocks_per_sm) {
+  if (!blocks_per_sm || threads < 32 || threads > kFusedMaxThreads)
+    return set_error(NZ_ERR_ARG, "nz_batch_occupancy: bad arguments");
+  return occupancy_fused(mode, threads, blocks_per_sm);
 }

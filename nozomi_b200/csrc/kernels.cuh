@@ -38,14 +38,15 @@ struct PlainArgs {
 __global__ void walk_plain_kernel(const PlainArgs a);
 
 // ---- fused walk (walk_fused.cu) ----
-constexpr int kFusedThreads = 128;
+constexpr int kFusedThreads = 128;     // walkers per CTA of nz_walk_fused
+constexpr int kFusedMaxThreads = 256;  // largest CTA of nz_walk_batch
 #ifndef NZ_FUSED_MIN_BLOCKS
-#define NZ_FUSED_MIN_BLOCKS 6
+#define NZ_FUSED_MIN_BLOCKS 3
 #endif
 #ifndef NZ_SCAN_BATCH
 #define NZ_SCAN_BATCH 4
 #endif
-constexpr int kFusedMinBlocks = NZ_FUSED_MIN_BLOCKS;  // CTAs per SM the register budget is sized for
+constexpr int kFusedMinBlocks = NZ_FUSED_MIN_BLOCKS;  // 256-thread CTAs per SM the register budget is sized for
 constexpr int kScanBatch = NZ_SCAN_BATCH;             // cell-list entries loaded together per thread
 constexpr int kMomentSteps = 256;  // steps per launch in NZ_MODE_MOMENTS (shared-memory staging)
 
@@ -81,7 +82,8 @@ struct JobDev {
 __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, const float* Garea, int nsteps, float dt,
                                     const nz_draws& d, int mode, const nz_state& st, double* moments);
 int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
-                 int step1, int* queue, int grid, cudaStream_t st);
+                 int step1, int* queue, int grid, int threads, cudaStream_t st);
+int occupancy_fused(int mode, int threads, int* blocks_per_sm);
 __global__ void pack_kernel(nz_walkers wk, const uint32_t* ids, nz_state st);
 __global__ void unpack_kernel(nz_state st, nz_walkers wk, int by_id, int* bad);
 

@@ -315,7 +315,7 @@ __device__ __forceinline__ void run_item(const JobDev& J, int first, int count, 
 // device arrays; with queue != null the grid is persistent and each CTA takes
 // items from *queue until none is left.
 template <int MODE, bool SINGLE>
-__global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
+__global__ void __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
     walk_fused_kernel(const __grid_constant__ JobDev single, const nz_job* __restrict__ jobs,
                       const nz_item* __restrict__ items, int n_items, int step0, int step1, int* queue) {
   __shared__ int s_item;
@@ -331,8 +331,8 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
     }
     if (it >= n_items) return;
     if (SINGLE) {
-      const int first = it * kFusedThreads;
-      const int count = min(kFusedThreads, single.nwalkers - first);
+      const int first = it * int(blockDim.x);
+      const int count = min(int(blockDim.x), single.nwalkers - first);
       run_item<MODE>(single, first, count, step0, step1, s_mom);
     } else {
       // every thread of the CTA works on the same job: its descriptor lives
@@ -437,7 +437,7 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
 
 template <int MODE>
 void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0, int step1,
-                 int* queue, int grid, cudaStream_t st) {
+                 int* queue, int grid, int threads, cudaStream_t st) {
   // the kernel keeps no data in shared memory: give the whole carveout to L1
   static bool configured = false;
   if (!configured) {
@@ -446,27 +446,46 @@ void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items,
     configured = true;
   }
   if (jobs)
-    walk_fused_kernel<MODE, false><<<grid, kFusedThreads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
+    walk_fused_kernel<MODE, false><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
   else
-    walk_fused_kernel<MODE, true><<<grid, kFusedThreads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
+    walk_fused_kernel<MODE, true><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
 }
 
 // jobs == null: the single job `single` with n_items CTAs of kFusedThreads walkers.
 int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
-                 int step1, int* queue, int grid, cudaStream_t st) {
+                 int step1, int* queue, int grid, int threads, cudaStream_t st) {
   switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS)) {
-    case NZ_MODE_PHI: launch_mode<NZ_MODE_PHI>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
-    case NZ_MODE_SIG: launch_mode<NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+    case NZ_MODE_PHI: launch_mode<NZ_MODE_PHI>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
+    case NZ_MODE_SIG: launch_mode<NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     case NZ_MODE_PHI | NZ_MODE_SIG:
-      launch_mode<NZ_MODE_PHI | NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+      launch_mode<NZ_MODE_PHI | NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     case NZ_MODE_SIG | NZ_MODE_MOMENTS:
-      launch_mode<NZ_MODE_SIG | NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+      launch_mode<NZ_MODE_SIG | NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     case NZ_MODE_MOMENTS:
-      launch_mode<NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
-    case 0: launch_mode<0>(single, jobs, items, n_items, step0, step1, queue, grid, st); break;
+      launch_mode<NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
+    case 0: launch_mode<0>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     default: return set_error(NZ_ERR_ARG, "fused walk: unsupported mode %d", mode);
   }
   return check_launch("walk_fused_kernel");
+}
+
+int occupancy_fused(int mode, int threads, int* blocks_per_sm) {
+  cudaError_t e;
+  switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS)) {
+    case NZ_MODE_PHI:
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<NZ_MODE_PHI, false>, threads, 0);
+      break;
+    case NZ_MODE_SIG:
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<NZ_MODE_SIG, false>, threads, 0);
+      break;
+    case NZ_MODE_PHI | NZ_MODE_SIG:
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm,
+                                                         walk_fused_kernel<NZ_MODE_PHI | NZ_MODE_SIG, false>, threads, 0);
+      break;
+    default: return set_error(NZ_ERR_ARG, "occupancy: unsupported batch mode %d", mode);
+  }
+  if (e != cudaSuccess) return set_error(NZ_ERR_CUDA, "occupancy: %s", cudaGetErrorString(e));
+  return NZ_OK;
 }
 
 }  // namespace nz

@@ -148,6 +148,27 @@ __global__ void __launch_bounds__(kSigThreads) signal_kernel(nz_state st, const 
   }
 }
 
+__global__ void __launch_bounds__(kSigThreads) signal_phase_kernel(const float* __restrict__ phase, int ndir, int N,
+                                                                   const float* __restrict__ amp, int nb,
+                                                                   double* __restrict__ out) {
+  __shared__ double s_red[32];
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = w < N;
+  for (int d = 0; d < ndir; ++d) {
+    const float ph = live ? phase[size_t(d) * N + w] : 0.f;
+    for (int b = 0; b < nb; ++b) {
+      float sn = 0.f, cs = 0.f;
+      if (live) sincosf(__ldg(amp + b) * ph, &sn, &cs);
+      const double re = block_sum(live ? double(cs) : 0.0, s_red);
+      const double im = block_sum(live ? double(sn) : 0.0, s_red);
+      if (threadIdx.x == 0) {
+        atomicAdd(out + d * nb + b, re);
+        atomicAdd(out + ndir * nb + d * nb + b, im);
+      }
+    }
+  }
+}
+
 __global__ void phase_from_phi_kernel(nz_state st, const float* __restrict__ dirs, int ndir, float* __restrict__ phase) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= st.N) return;
@@ -251,6 +272,16 @@ extern "C" int nz_signal_phi(const nz_state* st, const float* dirs, int ndir, co
   signal_kernel<<<(st->N + kSigThreads - 1) / kSigThreads, kSigThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       *st, dirs, ndir, amp, nb, out);
   return check_launch("signal_kernel");
+}
+
+extern "C" int nz_signal_phase(const float* phase, int ndir, int N, const float* amp, int nb, double* out,
+                               void* stream) {
+  if (!phase || !amp || !out || ndir <= 0 || nb <= 0 || N < 0)
+    return set_error(NZ_ERR_ARG, "nz_signal_phase: bad arguments");
+  if (N == 0) return NZ_OK;
+  signal_phase_kernel<<<(N + kSigThreads - 1) / kSigThreads, kSigThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      phase, ndir, N, amp, nb, out);
+  return check_launch("signal_phase_kernel");
 }
 
 extern "C" int nz_phase_from_phi(const nz_state* st, const float* dirs, int ndir, float* phase, void* stream) {

@@ -265,10 +265,15 @@ class FusedState:
     @staticmethod
     def from_walkers(wk: Walkers, ids: torch.Tensor | None = None) -> "FusedState":
         st = FusedState(wk.N)
-        s = st.struct()
+        st.pack(wk, ids)
+        return st
+
+    def pack(self, wk: Walkers, ids: torch.Tensor | None = None):
+        """Pack walkers (reference layout) into this state; walker ids are
+        ids[w], or w."""
+        s = self.struct()
         w = wk.struct()
         L.check(L.load().nz_state_pack(L.byref(w), _p(ids), L.byref(s), _stream()), "nz_state_pack")
-        return st
 
     def to_walkers(self, wk: Walkers):
         s = self.struct()

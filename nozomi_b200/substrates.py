@@ -152,16 +152,74 @@ def _bead_profile(r0, amp, phase, z, spacing, width=1.5):
     return r0[:, None] * (1.0 + amp[:, None] * np.exp(-d ** 2 / (2 * width ** 2)))
 
 
-def _required_distance(ri, rj, dz, max_shift=6):
-    """Smallest centre distance at which no sphere of axon i overlaps one of
-    axon j (both on the same z grid of step dz)."""
-    req = np.max(ri + rj)
-    for m in range(1, max_shift + 1):
-        for a, b in ((ri[:-m], rj[m:]), (ri[m:], rj[:-m])):
-            v = (a + b) ** 2 - (m * dz) ** 2
-            if v.size and v.max() > 0:
-                req = max(req, float(np.sqrt(v.max())))
+def _required_distances(R: np.ndarray, dz: float) -> np.ndarray:
+    """[n, n]: the smallest centre distance at which no sphere of axon i
+    overlaps one of axon j, for axons on the same z grid of step dz with
+    radius profiles R [n, k] (z-periodic profiles are compared cyclically)."""
+    n, k = R.shape
+    req = np.zeros((n, n))
+    rmax = R.max()
+    max_shift = min(k - 1, int(np.ceil(2 * rmax / dz)))
+    for m in range(0, max_shift + 1):
+        Rj = np.roll(R, -m, axis=1)
+        for a, b in ((R, Rj), (Rj, R)) if m else ((R, R),):
+            # (r_i[z] + r_j[z + m dz])^2 - (m dz)^2, maximised over z, in row blocks
+            for i0 in range(0, n, 64):
+                s2 = (a[i0:i0 + 64, None, :] + b[None, :, :]) ** 2 - (m * dz) ** 2
+                req[i0:i0 + 64] = np.maximum(req[i0:i0 + 64], np.sqrt(np.maximum(s2.max(-1), 0.0)))
     return req
+
+
+def _pack_centres(req: np.ndarray, box, rng, max_iter: int):
+    """Centres in a periodic 2-D box, pairwise distances >= req, by relaxing
+    overlaps from random positions (minimum-image)."""
+    n = req.shape[0]
+    Lx, Ly = box
+    # start from a jittered grid in random order: few overlaps to relax
+    nx = max(1, int(np.ceil(np.sqrt(n * Lx / Ly))))
+    ny = max(1, int(np.ceil(n / nx)))
+    gx, gy = np.meshgrid((np.arange(nx) + 0.5) * Lx / nx - Lx / 2, (np.arange(ny) + 0.5) * Ly / ny - Ly / 2)
+    cells = rng.permutation(nx * ny)[:n]
+    P = np.stack([gx.ravel()[cells], gy.ravel()[cells]], axis=1)
+    P += rng.uniform(-0.25, 0.25, P.shape) * np.array([Lx / nx, Ly / ny])
+    b = np.array([Lx, Ly])
+    req = req.copy()
+    np.fill_diagonal(req, 0.0)
+    worst = np.inf
+    for it in range(max_iter):
+        d = P[:, None, :] - P[None, :, :]
+        d -= b * np.round(d / b)
+        dist = np.sqrt((d ** 2).sum(-1)) + np.eye(n)
+        ov = np.maximum(0.0, req - dist)
+        np.fill_diagonal(ov, 0.0)
+        worst = ov.max()
+        if worst < 1e-9:
+            return P, it
+        P += ((ov / dist)[:, :, None] * d * 0.5).sum(1)
+        P = (P + b / 2) % b - b / 2
+    raise RuntimeError(f"packing did not converge (largest overlap {worst:.3g} um)")
+
+
+def _axons_with_images(P, R, z, L, image_margin):
+    Lx, Ly, Lz = L
+    dz = z[1] - z[0]
+    fibers = []
+    rmax = R.max(1)
+    for i in range(P.shape[0]):
+        base = np.stack([np.full(z.size, P[i, 0]), np.full(z.size, P[i, 1]), z, R[i]], axis=1)
+        nimg = int(np.ceil((rmax[i] + image_margin) / dz)) + 1
+        zimg = np.concatenate([base[-nimg:] - [0, 0, Lz, 0], base, base[:nimg] + [0, 0, Lz, 0]])
+        parts = [zimg]
+        reach = rmax[i] + image_margin
+        sx = [0.0] + ([Lx] if P[i, 0] - reach < -Lx / 2 else []) + ([-Lx] if P[i, 0] + reach > Lx / 2 else [])
+        sy = [0.0] + ([Ly] if P[i, 1] - reach < -Ly / 2 else []) + ([-Ly] if P[i, 1] + reach > Ly / 2 else [])
+        for ox in sx:
+            for oy in sy:
+                if ox == 0.0 and oy == 0.0:
+                    continue
+                parts.append(zimg + [ox, oy, 0.0, 0.0])
+        fibers.append(np.concatenate(parts))
+    return fibers
 
 
 def packed_axons(n_axons: int = 200, L=(40.0, 40.0, 80.0), spheres_per_axon: int = 100, r_mean: float = 1.0,
@@ -177,50 +235,31 @@ def packed_axons(n_axons: int = 200, L=(40.0, 40.0, 80.0), spheres_per_axon: int
     amp = rng.uniform(bead_amp[0], bead_amp[1], n_axons)
     phase = rng.uniform(0, bead_spacing, n_axons)
     R = _bead_profile(r0, amp, phase, z, bead_spacing)               # [n, k]
-    # required centre distances
-    req = np.zeros((n_axons, n_axons))
-    for i in range(n_axons):
-        for j in range(i + 1, n_axons):
-            req[i, j] = req[j, i] = _required_distance(R[i], R[j], dz) + gap
-    # relaxation from random centres (minimum-image, periodic in x and y)
-    P = np.stack([rng.uniform(-Lx / 2, Lx / 2, n_axons), rng.uniform(-Ly / 2, Ly / 2, n_axons)], axis=1)
-    box = np.array([Lx, Ly])
-    np.fill_diagonal(req, 0.0)
-    for it in range(max_iter):
-        d = P[:, None, :] - P[None, :, :]
-        d -= box * np.round(d / box)
-        dist = np.sqrt((d ** 2).sum(-1)) + np.eye(n_axons)
-        ov = np.maximum(0.0, req - dist)
-        np.fill_diagonal(ov, 0.0)
-        worst = ov.max()
-        if worst < 1e-9:
-            break
-        push = (ov / dist)[:, :, None] * d * 0.5
-        P += push.sum(1)
-        P = (P + box / 2) % box - box / 2
-    else:
-        raise RuntimeError(f"packing did not converge (largest overlap {worst:.3g} um)")
-    fibers = []
-    rmax = R.max(1)
-    for i in range(n_axons):
-        base = np.stack([np.full(z.size, P[i, 0]), np.full(z.size, P[i, 1]), z, R[i]], axis=1)
-        # z-periodic images: enough spheres to cover image_margin beyond each z face
-        nimg = int(np.ceil((rmax[i] + image_margin) / dz)) + 1
-        zimg = np.concatenate([base[-nimg:] - [0, 0, Lz, 0], base, base[:nimg] + [0, 0, Lz, 0]])
-        parts = [zimg]
-        reach = rmax[i] + image_margin
-        sx = [0.0] + ([Lx] if P[i, 0] - reach < -Lx / 2 else []) + ([-Lx] if P[i, 0] + reach > Lx / 2 else [])
-        sy = [0.0] + ([Ly] if P[i, 1] - reach < -Ly / 2 else []) + ([-Ly] if P[i, 1] + reach > Ly / 2 else [])
-        for ox in sx:
-            for oy in sy:
-                if ox == 0.0 and oy == 0.0:
-                    continue
-                parts.append(zimg + [ox, oy, 0.0, 0.0])
-        fibers.append(np.concatenate(parts))
+    req = _required_distances(R, dz) + gap
+    P, it = _pack_centres(req, (Lx, Ly), rng, max_iter)
+    fibers = _axons_with_images(P, R, z, (Lx, Ly, Lz), image_margin)
     vf = float(np.mean([np.pi * (R[:, k] ** 2).sum() for k in range(z.size)]) / (Lx * Ly))
     return Substrate(fibers, (Lx, Ly, Lz), {"kind": "packed_axons", "n_axons": n_axons, "seed": seed,
                                              "centres": P, "r0": r0, "amp": amp, "bead_phase": phase,
                                              "volume_fraction": vf, "relax_iterations": it})
+
+
+def axon_bundle(n_axons: int, seed: int, spheres_per_axon: int = 40, Lz: float = 40.0, r_range=(0.5, 1.5),
+                area_fraction: float = 0.35, gap: float = 0.05, image_margin: float = 2.0) -> Substrate:
+    """n beaded axons built like the single axon of ``beaded_axon`` (spheres at
+    Lz / n spacing, radii uniform in r_range, z-periodic), packed without
+    overlap in a square periodic box sized for the given mean cross-section
+    area fraction."""
+    rng = np.random.default_rng(seed)
+    dz = Lz / spheres_per_axon
+    z = -Lz / 2 + dz / 2 + dz * np.arange(spheres_per_axon)
+    R = rng.uniform(r_range[0], r_range[1], (n_axons, spheres_per_axon))
+    side = float(np.sqrt(np.pi * (R ** 2).mean(1).sum() / area_fraction))
+    req = _required_distances(R, dz) + gap
+    P, it = _pack_centres(req, (side, side), rng, 20000)
+    fibers = _axons_with_images(P, R, z, (side, side, Lz), image_margin)
+    return Substrate(fibers, (side, side, Lz), {"kind": "axon_bundle", "n_axons": n_axons, "seed": seed,
+                                                 "relax_iterations": it})
 
 
 def cell_grid(L, cell: float):

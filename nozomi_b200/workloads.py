@@ -1,0 +1,106 @@
+"""Synthetic mixed workloads (seeded): many beaded-axon substrates of uneven
+size under per-substrate PGSE protocols.
+
+* ``mixed_specs`` — the batched workload: substrates built like the single
+  beaded axon (40 spheres at 1 um, radii U[0.5, 1.5], z-periodic) but with
+  axon counts uniform in [10, 500] packed in a periodic box; walker counts
+  log-uniform in [1e4, 1e6] (rounded to 1000); step counts uniform in
+  [2000, 8000] at dt = 5 us with PGSE delta = te/3, Delta = 2 te/3; 6 to 60
+  directions uniform on the sphere; b in {0, 1, 2, 3} ms/um^2.
+* ``request_stream`` — the served workload: Poisson arrivals; each request
+  draws a substrate from the same distribution (an earlier one again with
+  probability 0.7), 1e4 to 5e5 walkers log-uniform, 6 to 60 directions,
+  b up to 3 ms/um^2.
+Substrates are cached on disk under ~/.cache/nozomi_b200 (they take seconds
+to pack).
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import pickle
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from .batch import JobSpec
+from .substrates import Substrate, axon_bundle
+from .waveforms import PGDiffWaveform
+
+CACHE = Path(os.environ.get("NOZOMI_B200_CACHE", Path.home() / ".cache" / "nozomi_b200"))
+DT = 0.005
+
+
+def bundle(n_axons: int, seed: int) -> Substrate:
+    CACHE.mkdir(parents=True, exist_ok=True)
+    key = hashlib.sha1(f"axon_bundle-v1-{n_axons}-{seed}".encode()).hexdigest()[:16]
+    path = CACHE / f"bundle_{key}.pkl"
+    if path.exists():
+        with open(path, "rb") as f:
+            return pickle.load(f)
+    s = axon_bundle(n_axons, seed)
+    tmp = path.with_suffix(".tmp")
+    with open(tmp, "wb") as f:
+        pickle.dump(s, f)
+    os.replace(tmp, path)
+    return s
+
+
+def pgse(steps: int, dt: float = DT) -> PGDiffWaveform:
+    te = steps * dt
+    return PGDiffWaveform(2 * te / 3, te / 3, te, time_step=dt)
+
+
+def unit_directions(rng, n: int) -> np.ndarray:
+    d = rng.standard_normal((3, n))
+    return d / np.linalg.norm(d, axis=0)
+
+
+def mixed_specs(seed: int = 4, n_jobs: int = 64, axons=(10, 500), walkers=(1e4, 1e6), steps=(2000, 8000),
+                ndirs=(6, 60), bvalues=(0.0, 1.0, 2.0, 3.0), walker_scale: float = 1.0) -> list:
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_jobs):
+        na = int(rng.integers(axons[0], axons[1] + 1))
+        N = int(max(1000, round(np.exp(rng.uniform(np.log(walkers[0]), np.log(walkers[1]))) * walker_scale / 1000)
+                    * 1000))
+        nst = int(rng.integers(steps[0], steps[1] + 1))
+        nd = int(rng.integers(ndirs[0], ndirs[1] + 1))
+        gw = pgse(nst)
+        dirs = unit_directions(rng, nd)
+        amps = gw.amplitude_for_b(np.asarray(bvalues))
+        specs.append(JobSpec(bundle(na, seed * 1000 + i), gw, dirs, amps, N, seed=seed * 100000 + i,
+                             key=("bundle", na, seed * 1000 + i)))
+    return specs
+
+
+@dataclass
+class Request:
+    arrival: float       # seconds after the stream starts
+    spec: JobSpec
+
+
+def request_stream(rate: float, duration: float, seed: int = 5, reuse: float = 0.7, axons=(10, 500),
+                   walkers=(1e4, 5e5), steps=(2000, 8000), ndirs=(6, 60), bmax: float = 3.0,
+                   max_requests: int | None = None) -> list:
+    rng = np.random.default_rng(seed)
+    t, out, seen = 0.0, [], []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration or (max_requests is not None and len(out) >= max_requests):
+            break
+        if seen and rng.uniform() < reuse:
+            na, sseed = seen[int(rng.integers(len(seen)))]
+        else:
+            na, sseed = int(rng.integers(axons[0], axons[1] + 1)), int(rng.integers(1 << 30))
+            seen.append((na, sseed))
+        N = int(max(1000, round(np.exp(rng.uniform(np.log(walkers[0]), np.log(walkers[1]))) / 1000) * 1000))
+        nst = int(rng.integers(steps[0], steps[1] + 1))
+        nd = int(rng.integers(ndirs[0], ndirs[1] + 1))
+        gw = pgse(nst)
+        b = np.linspace(0.0, rng.uniform(1.0, bmax), 4)
+        spec = JobSpec(bundle(na, sseed), gw, unit_directions(rng, nd), gw.amplitude_for_b(b), N,
+                       seed=int(rng.integers(1 << 31)), key=("bundle", na, sseed))
+        out.append(Request(t, spec))
+    return out
