@@ -53,8 +53,12 @@ def parse():
     ap.add_argument("--coarsen", type=int, default=None)
     ap.add_argument("--by-label", type=int, default=None, help="re-bin by (label, bin): 1, or by bin only: 0")
     ap.add_argument("--near-margin", type=float, default=None, help="near-list margin in um (0: none)")
-    ap.add_argument("--workload", default="packed", choices=["packed", "batched"],
-                    help="packed: one packed substrate (default); batched: 64 mixed substrates, batched vs plain")
+    ap.add_argument("--workload", default="packed", choices=["packed", "batched", "serving"],
+                    help="packed: one packed substrate (default); batched: 64 mixed substrates, batched vs plain; "
+                         "serving: Poisson request streams, continuous batching, p50/p99 latency")
+    ap.add_argument("--rates", default="5,20,50,100,200", help="serving: request rates (req/s)")
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="serving: arrival window per rate")
+    ap.add_argument("--max-requests", type=int, default=200, help="serving: requests per rate at most")
     ap.add_argument("--jobs", type=int, default=64, help="batched: number of substrates")
     ap.add_argument("--walker-scale", type=float, default=1.0, help="batched: scale of the walker counts")
     ap.add_argument("--threads", type=int, default=128, help="batched: walkers per CTA")
@@ -472,12 +476,84 @@ def run_batched(args):
     return 0
 
 
+def run_serving(args):
+    import torch
+    from nozomi_b200 import engine
+    from nozomi_b200.batch import SubstrateCache
+    from nozomi_b200.plain import run_plain
+    from nozomi_b200.serve import Server, latency_stats
+    from nozomi_b200.simulate import Tuning
+    from nozomi_b200.workloads import request_stream
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    engine.require_cuda()
+    tuning = Tuning()
+    if args.steps_per_launch:
+        tuning.steps_per_launch = args.steps_per_launch
+    cache = SubstrateCache()
+    per_rate = []
+    all_done = []
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    for rate in [float(r) for r in args.rates.split(",")]:
+        reqs = request_stream(rate, min(args.serve_seconds, args.max_requests / rate), seed=5,
+                              max_requests=args.max_requests)
+        # warm the substrate cache's first entries so every rate starts from the same state
+        srv = Server(tuning=tuning, threads=args.threads, cache=cache)
+        t0 = time.perf_counter()
+        done = srv.serve(reqs)
+        wall = time.perf_counter() - t0
+        st = latency_stats(done)
+        st.update({"rate_req_s": rate, "requests": len(reqs), "walker_steps": srv.walker_steps,
+                   "walker_steps_per_s": srv.walker_steps / wall, "wall_s": wall, "rounds": srv.rounds,
+                   "failed": sum(t.error is not None for t in done)})
+        per_rate.append(st)
+        all_done += done
+    clk = clocks.stop()
+    # the plain per-substrate kernel on a sample of the same requests, one after another
+    sample = all_done[:: max(1, len(all_done) // 8)][:8]
+    stream = torch.cuda.current_stream()
+    pms, pws = 0.0, 0
+    for t in sample:
+        sp = t.spec
+        dsub = cache.get(sp.key, sp.substrate, sp.D, sp.T2, tuning)
+        x, _ = engine.seed(dsub, list(range(dsub.nstructures + 1)), sp.N, key=sp.seed ^ 0x5EED)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run_plain(dsub, sp, x)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms += e0.elapsed_time(e1)
+        pws += sp.N * sp.nsteps
+    plain_value = pws / (pms * 1e-3)
+    total_ws = sum(r["walker_steps"] for r in per_rate)
+    total_wall = sum(r["wall_s"] for r in per_rate)
+    value = total_ws / total_wall
+    line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
+            "steps": len(per_rate), "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded Poisson request streams)",
+            "config": {"workload": "serving: Poisson arrivals per rate, substrates of 10-500 beaded axons reused "
+                                   "with probability 0.7, 1e4-5e5 walkers, 2000-8000 steps at 5 us, 6-60 directions, "
+                                   "b<=3 ms/um^2, seed 5", "rates": args.rates,
+                       "arrival_window_s": args.serve_seconds, "max_requests_per_rate": args.max_requests,
+                       "steps_per_launch": tuning.steps_per_launch, "threads": args.threads},
+            "per_rate": per_rate,
+            "plain": {"value": plain_value, "unit": "walker-steps/s", "requests_timed": len(sample),
+                      "launch": "one plain-kernel launch per step, requests one after another"},
+            "speedup_vs_plain": value / plain_value, "substrate_cache": {"hits": cache.hits, "misses": cache.misses},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "serving":
+        return run_serving(args)
     return run_ours(args)
 
 

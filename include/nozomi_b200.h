@@ -129,6 +129,7 @@ typedef struct nz_job {
     int mode;              /* NZ_MODE_PHI and/or NZ_MODE_SIG */
     nz_state state;
     double* moments;       /* [nsteps][6] (NZ_MODE_MOMENTS) or NULL */
+    int step_offset;       /* this job runs steps [step0 + step_offset, step1 + step_offset) of a launch */
 } nz_job;
 
 /* A work item: walkers [first, first + count) of job `job`, count <= block size. */

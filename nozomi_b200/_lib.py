@@ -50,7 +50,7 @@ class State(ctypes.Structure):
 
 class Job(ctypes.Structure):
     _fields_ = [("sub", Substrate), ("G", _P), ("Garea", _P), ("nsteps", _i), ("dt", _f), ("draws", Draws),
-                ("mode", _i), ("state", State), ("moments", _P)]
+                ("mode", _i), ("state", State), ("moments", _P), ("step_offset", _i)]
 
 
 class Item(ctypes.Structure):

@@ -96,6 +96,7 @@ def _job_table(jobs, states) -> torch.Tensor:
         arr[i].mode = L.MODE_PHI
         arr[i].state = st.struct()
         arr[i].moments = None
+        arr[i].step_offset = int(j.get("offset", 0))
     raw = np.frombuffer(bytes(arr), dtype=np.uint8).copy()
     return torch.from_numpy(raw).cuda()
 

@@ -71,6 +71,7 @@ struct JobDev {
   float4* comp;
   double* moments;
   int nwalkers;
+  int step_offset;
   // near lists (null sph4: none)
   float near_margin;
   const int* near_start;

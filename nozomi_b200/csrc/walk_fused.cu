@@ -295,7 +295,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
 // clamped to the job's protocol.
 template <int MODE>
 __device__ __forceinline__ void run_item(const JobDev& J, int first, int count, int step0, int step1, float* s_mom) {
-  const int s0 = step0, s1 = min(step1, J.nsteps);
+  const int s0 = step0 + J.step_offset, s1 = min(step1 + J.step_offset, J.nsteps);
   if (MODE & NZ_MODE_MOMENTS) {
     for (int i = threadIdx.x; i < kMomentSteps * 6; i += blockDim.x) s_mom[i] = 0.0f;
     __syncthreads();
@@ -341,6 +341,7 @@ __global__ void __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
       if (threadIdx.x == 0) {
         const nz_job& a = jobs[wi.job];
         s_job = make_job(a.sub, a.G, a.Garea, a.nsteps, a.dt, a.draws, a.mode, a.state, a.moments);
+        s_job.step_offset = a.step_offset;
       }
       __syncthreads();
       run_item<MODE>(s_job, wi.first, wi.count, step0, step1, s_mom);
@@ -405,6 +406,7 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
                                     const nz_draws& d, int mode, const nz_state& st, double* moments) {
   JobDev j;
   j.nwalkers = st.N;
+  j.step_offset = 0;
   j.g = Grid{sub.grid.Lx, sub.grid.Ly, sub.grid.Lz, sub.grid.dLx, sub.grid.dLy, sub.grid.dLz,
              float(sub.grid.nx), float(sub.grid.ny), float(sub.grid.nz)};
   j.nstructures = sub.nstructures;
