@@ -21,6 +21,7 @@ workload.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import subprocess
@@ -63,6 +64,7 @@ def parse():
     ap.add_argument("--walker-scale", type=float, default=1.0, help="batched: scale of the walker counts")
     ap.add_argument("--threads", type=int, default=128, help="batched: walkers per CTA")
     ap.add_argument("--plain-every", type=int, default=1, help="batched: time the plain path on every k-th job")
+    ap.add_argument("--autotune", action="store_true", help="batched: pick the launch shape with the autotuner")
     return ap.parse_args()
 
 
@@ -202,7 +204,8 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     from nozomi_b200 import engine, _lib as L
-    from nozomi_b200.simulate import DwiRun, Tuning, device_substrate
+    from nozomi_b200.shard import ShardedDwiRun, reduce_sums
+    from nozomi_b200.simulate import Tuning, device_substrate
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -227,7 +230,10 @@ def run_ours(args):
     dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin)
     amps = pg.amplitude_for_b(bvals)
     N = args.walkers
-    run = DwiRun(dsub, pg, dirs, amps, N, seed=1000 + rank, tuning=tuning)
+    # walkers [rank*N, (rank+1)*N) of one run of N*world walkers; the signal
+    # sums are all-reduced once per step (the path's one exchange)
+    shard = ShardedDwiRun(dsub, pg, dirs, amps, N * world, seed=1000, rank=rank, world=world, tuning=tuning)
+    run = shard.run
     x0, lab0 = run.initial_positions()
     flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     stream = torch.cuda.current_stream()
@@ -280,6 +286,7 @@ def run_ours(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         graph.replay()
+        reduce_sums(sig_static)
         e1.record(stream)
         torch.cuda.synchronize()
         step_ms += e0.elapsed_time(e1)
@@ -309,7 +316,7 @@ def run_ours(args):
     ws_per_step = N * run.nsteps * world
     value = ws_per_step * args.steps / (step_ms * 1e-3)
     S = sig.cpu().numpy()
-    S = (S[0] + 1j * S[1]) / N
+    S = (S[0] + 1j * S[1]) / (N * world)
 
     # end to end with host buffers: positions copied from pinned host memory
     # into the graph's input, the step replayed, the signal copied back
@@ -323,6 +330,7 @@ def run_ours(args):
         e0.record(stream)
         x0.copy_(x_host, non_blocking=True)
         graph.replay()
+        reduce_sums(sig_static)
         host.copy_(sig_static, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -375,7 +383,8 @@ def run_ours(args):
                            "near_list_entries": int(dsub.near[2].numel()) if dsub.near is not None else 0,
                            "spheres": sub.S, "cells": dsub.ncell,
                            "cell_list_entries": dsub.n_items, "l2": "256 MiB flush between timed steps",
-                           "parallelism": f"walkers sharded over {world} GPU(s)"},
+                           "parallelism": f"walkers sharded over {world} GPU(s) by walker-id range; "
+                                          "one all-reduce of the signal sums per step"},
                 "e2e": {"value": e2e_value, "unit": "walker-steps/s",
                         "h2d_bytes_per_step": int(x_host.numel() * x_host.element_size()),
                         "d2h_bytes_per_step": int(out_bytes)},
@@ -416,8 +425,13 @@ def run_batched(args):
         tuning.steps_per_launch = args.steps_per_launch
     if args.near_margin is not None:
         tuning.near_margin = args.near_margin if args.near_margin > 0 else None
+    tune_report = None
+    threads = args.threads
+    if args.autotune:
+        from nozomi_b200.autotune import autotune
+        tuning, threads, tune_report = autotune(specs)
     cache = SubstrateCache()
-    run = BatchRun(specs, tuning=tuning, threads=args.threads, cache=cache)
+    run = BatchRun(specs, tuning=tuning, threads=threads, cache=cache)
     stream = torch.cuda.current_stream()
     run.step()
     for _ in range(max(0, args.warmup - 1)):
@@ -463,9 +477,14 @@ def run_batched(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded substrates, protocols and walkers)",
             "config": {"workload": BATCH_WORKLOAD.format(jobs=len(specs), scale=args.walker_scale),
-                       "jobs": len(specs), "walker_steps_per_step": ws, "threads": args.threads,
+                       "jobs": len(specs), "walker_steps_per_step": ws, "threads": threads,
                        "steps_per_launch": tuning.steps_per_launch, "near_margin_um": tuning.near_margin,
+                       "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen,
                        "persistent_grid": run.grid, "chunks": len(run.chunks)},
+            "autotune": None if tune_report is None else {
+                "cached": tune_report["cached"], "choice": {"threads": threads, **dataclasses.asdict(tuning)},
+                "trials": len(tune_report.get("trials", [])),
+                "trial_walker_steps_per_s": tune_report.get("trial_walker_steps_per_s")},
             "gpu_launches": run.launches() * args.steps,
             "plain": {"value": plain_value, "unit": "walker-steps/s", "jobs_timed": len(sel),
                       "walker_steps_timed": plain_ws, "launch": "one plain-kernel launch per step from the host, "

@@ -37,6 +37,8 @@ extern "C" {
 #define NZ_MODE_PHASE 2     /* per-direction phase[ndir][N] (randomWalk3d_phase_multidirr) */
 #define NZ_MODE_PHI 4       /* Kahan 3-vector Phi = sum_n G_n p_n; phase_d = u_d . Phi */
 #define NZ_MODE_MOMENTS 8   /* per-step displacement moments (fused walk only) */
+#define NZ_MODE_TANGENT64 16 /* fused walk: a solve whose normalised discriminant sqterm/4a is below
+                                1e-6 um^2 (a near-tangent ray) is recomputed in FP64 */
 
 /* per-walker flag bits */
 #define NZ_FLAG_DRAWS_EXHAUSTED 1
@@ -183,6 +185,14 @@ int nz_cells_gather(const float* spheres, int S, const int* items, int n_items, 
  * n_unseeded: one device int.  Returns NZ_OK; check *n_unseeded on the host. */
 int nz_seed(const nz_substrate* sub, const uint8_t* target, int N, uint32_t key0, uint32_t key1,
             uint32_t stream_id, int max_rounds, float* spins, int* label, int* n_unseeded, void* stream);
+
+/* Walkers [id0, id0 + N) of the same seeding into slots [0, N): a shard of a
+ * run sharded over processes seeds exactly its walkers of the unsharded run.
+ * No reference counterpart (the reference runs one process per GPU with
+ * independent seeds); nz_seed is this with id0 = 0.  id0 + N <= 2^32. */
+int nz_seed_range(const nz_substrate* sub, const uint8_t* target, uint32_t id0, int N, uint32_t key0,
+                  uint32_t key1, uint32_t stream_id, int max_rounds, float* spins, int* label, int* n_unseeded,
+                  void* stream);
 
 /* ---- a3/a4/a5: one time step of every walker, one launch —
  * randomWalk3d (sim3d_kernel.cu:340-522), randomWalk3d_phase (:524-717),

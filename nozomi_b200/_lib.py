@@ -11,7 +11,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libnozomi_b200.so"
 
 NZ_OK, NZ_ERR_ARG, NZ_ERR_CUDA, NZ_ERR_CAPACITY, NZ_ERR_UNSEEDED = 0, 1, 2, 3, 4
-MODE_SIG, MODE_PHASE, MODE_PHI, MODE_MOMENTS = 1, 2, 4, 8
+MODE_SIG, MODE_PHASE, MODE_PHI, MODE_MOMENTS, MODE_TANGENT64 = 1, 2, 4, 8, 16
 FLAG_DRAWS_EXHAUSTED, FLAG_ITER_CAP, FLAG_UNSEEDED = 1, 2, 4
 FUSED_THREADS = 128       # walkers per CTA / per work item of the fused and batched walks
 MOMENT_STEPS = 256        # steps per launch when the fused walk accumulates moments
@@ -69,6 +69,7 @@ SIGNATURES = {
     "nz_segments_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _i, _P, _P]),
     "nz_cells_gather": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _P, _P]),
     "nz_seed": (_i, [_P, _P, _i, _u, _u, _u, _i, _P, _P, _P, _P]),
+    "nz_seed_range": (_i, [_P, _P, _u, _i, _u, _u, _u, _i, _P, _P, _P, _P]),
     "nz_walk_step": (_i, [_P, _P, _i, _f, _f, _f, _i, _P, _P]),
     "nz_state_pack": (_i, [_P, _P, _P, _P]),
     "nz_state_unpack": (_i, [_P, _P, _P]),

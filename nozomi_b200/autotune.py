@@ -1,0 +1,115 @@
+"""Launch-shape autotuner for the batched walk.
+
+Chooses walkers per CTA (``threads``), cell edge, near-list margin, steps per
+launch and re-binning coarsening by timing short trials of the batch itself:
+at most ``max_jobs`` jobs (the largest), each cut to ``max_walkers`` walkers
+and its first ``trial_steps`` steps.  The search is coordinate descent from
+the defaults, one parameter at a time, keeping a change only if it is faster
+by more than ``min_gain``.  Choices are cached per (GPU, workload signature)
+in a JSON file so later runs of the same shape skip the search.
+"""
+from __future__ import annotations
+
+import dataclasses
+import hashlib
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from .batch import BatchRun, JobSpec, SubstrateCache
+from .simulate import Tuning
+from .waveforms import ArbitraryWaveform
+
+SPACE = {
+    "threads": [64, 128, 256],
+    "cell": [1.0, 1.5],
+    "near_margin": [0.4, 0.5, 0.6, None],
+    "steps_per_launch": [250, 500, 1000, 2000],
+    "coarsen": [2, 4, 8],
+}
+CACHE_FILE = Path(os.environ.get("NOZOMI_B200_CACHE", Path.home() / ".cache" / "nozomi_b200")) / "autotune.json"
+
+
+def signature(specs) -> str:
+    """Workload shape: job count, walker/step/direction/sphere-count histograms, dt."""
+    N = np.array([s.N for s in specs])
+    st = np.array([s.nsteps for s in specs])
+    nd = np.array([np.asarray(s.dirs).shape[1] for s in specs])
+    S = np.array([s.substrate.S for s in specs])
+    dts = sorted({round(float(s.gwave.dt), 6) for s in specs})
+    q = lambda a: np.percentile(a, [10, 50, 90]).round(-2 if a.max() > 1000 else 0).tolist()  # noqa: E731
+    key = json.dumps({"n": len(specs), "N": q(N), "steps": q(st), "dirs": q(nd), "S": q(S), "dt": dts})
+    gpu = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+    return hashlib.sha1((gpu + key).encode()).hexdigest()[:16]
+
+
+def _trial_specs(specs, max_jobs, max_walkers, trial_steps):
+    big = sorted(specs, key=lambda s: -s.walker_steps)[:max_jobs]
+    out = []
+    for s in big:
+        w = np.asarray(s.gwave.wave)[:trial_steps]
+        gw = ArbitraryWaveform(w, s.gwave.dt)
+        out.append(dataclasses.replace(s, gwave=gw, N=min(s.N, max_walkers)))
+    return out
+
+
+def _time(specs, tuning, threads, cache, reps=2) -> float:
+    run = BatchRun(specs, tuning=tuning, threads=threads, cache=cache)
+    run.step()  # warm-up: allocations, cell lists, scratch
+    stream = torch.cuda.current_stream()
+    best = float("inf")
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run.step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return run.walker_steps() / (best * 1e-3)
+
+
+def autotune(specs, space=None, trial_steps: int = 2000, max_walkers: int = 50_000, max_jobs: int = 16,
+             min_gain: float = 0.02, use_cache: bool = True, cache_file: Path = CACHE_FILE):
+    """Returns (Tuning, threads, report)."""
+    space = space or SPACE
+    sig = signature(specs)
+    if use_cache and cache_file.exists():
+        saved = json.loads(cache_file.read_text()).get(sig)
+        if saved:
+            t = Tuning(**saved["tuning"])
+            return t, saved["threads"], {"cached": True, "signature": sig, **saved}
+    trial = _trial_specs(specs, max_jobs, max_walkers, trial_steps)
+    cache = SubstrateCache()
+    cur = {"threads": 128, "cell": 1.0, "near_margin": 0.5, "steps_per_launch": 500, "coarsen": 4}
+    trials = []
+
+    def measure(cfg):
+        t = Tuning(cell=cfg["cell"], near_margin=cfg["near_margin"], steps_per_launch=cfg["steps_per_launch"],
+                   coarsen=cfg["coarsen"])
+        v = _time(trial, t, cfg["threads"], cache)
+        trials.append({**cfg, "walker_steps_per_s": v})
+        return v
+
+    best = measure(cur)
+    for name in ["near_margin", "threads", "steps_per_launch", "coarsen", "cell"]:
+        for val in space[name]:
+            if val == cur[name]:
+                continue
+            cand = dict(cur, **{name: val})
+            v = measure(cand)
+            if v > best * (1 + min_gain):
+                best, cur = v, cand
+    tuning = Tuning(cell=cur["cell"], near_margin=cur["near_margin"], steps_per_launch=cur["steps_per_launch"],
+                    coarsen=cur["coarsen"])
+    report = {"cached": False, "signature": sig, "tuning": dataclasses.asdict(tuning), "threads": cur["threads"],
+              "trial_walker_steps_per_s": best, "trials": trials}
+    if use_cache:
+        cache_file.parent.mkdir(parents=True, exist_ok=True)
+        data = json.loads(cache_file.read_text()) if cache_file.exists() else {}
+        data[sig] = {"tuning": report["tuning"], "threads": cur["threads"], "trial_walker_steps_per_s": best}
+        cache_file.write_text(json.dumps(data, indent=1))
+    return tuning, cur["threads"], report

@@ -224,6 +224,66 @@ __device__ __forceinline__ float step_out(float dx, float dy, float dz, float r,
 // rounding host expf and does not drift over many steps.
 __device__ __forceinline__ float t2_decay(float x) { return float(exp(double(x))); }
 
+// FP64 forms of the two fractions, for near-tangent rays (the chosen
+// precision form): the same rule evaluated in double from the float inputs.
+__device__ __forceinline__ double step_in_f64(double dx, double dy, double dz, double r, double jx, double jy,
+                                              double jz) {
+  const double tol = double(kTol);
+  if ((dx * dx + dy * dy + dz * dz - r * r) > 0) return 1e6;  // the inside test, redone in double
+  const double a = jx * jx + jy * jy + jz * jz;
+  const double b = 2 * (jx * dx + jy * dy + jz * dz);
+  const double c = dx * dx + dy * dy + dz * dz - (r - tol) * (r - tol);
+  double sq = b * b - 4 * a * c;
+  if (sq < 0) return 0;
+  sq = sqrt(sq);
+  double q = -0.5 * (b + sq);
+  if (b < 0) q = -0.5 * (b - sq);
+  const double fpos = q / a, fneg = c / q;
+  const double m = (fpos < fneg) ? fneg : fpos;
+  return (m < 0) ? 0 : m;
+}
+__device__ __forceinline__ double step_out_f64(double dx, double dy, double dz, double r, double jx, double jy,
+                                               double jz) {
+  const double tol = double(kTol);
+  const double a = jx * jx + jy * jy + jz * jz;
+  const double b = 2 * (jx * dx + jy * dy + jz * dz);
+  const double c = dx * dx + dy * dy + dz * dz - (r + tol) * (r + tol);
+  double sq = b * b - 4 * a * c;
+  if (sq < 0) return 1e6;
+  sq = sqrt(sq);
+  double q = -0.5 * (b + sq);
+  if (b < 0) q = -0.5 * (b - sq);
+  const double fpos = q / a, fneg = c / q;
+  if ((dx * dx + dy * dy + dz * dz - r * r) < 0) return (fpos < fneg) ? fneg : fpos;  // inside, in double
+  if (fpos > 0 && fneg > 0) return (fpos > fneg) ? fneg : fpos;
+  else if ((fpos < 0 && fneg < 0) || (b > 0)) return 1e6;
+  return 0;
+}
+
+// The reference fractions with the near-tangent FP64 form when T64.
+template <bool T64>
+__device__ __forceinline__ float step_in_t(float dx, float dy, float dz, float r, float a, float jx, float jy,
+                                           float jz) {
+  if (T64) {
+    const float b = 2 * (jx * dx + jy * dy + jz * dz);
+    const float c = dx * dx + dy * dy + dz * dz - (r - kTol) * (r - kTol);
+    const float sq = b * b - 4 * a * c;
+    if (sq < __uint_as_float(0x368637bdu) * a) return float(step_in_f64(dx, dy, dz, r, jx, jy, jz));  // 4e-6
+  }
+  return step_in(dx, dy, dz, r, a, jx, jy, jz);
+}
+template <bool T64>
+__device__ __forceinline__ float step_out_t(float dx, float dy, float dz, float r, float a, float jx, float jy,
+                                            float jz) {
+  if (T64) {
+    const float b = 2 * (jx * dx + jy * dy + jz * dz);
+    const float c = dx * dx + dy * dy + dz * dz - (r + kTol) * (r + kTol);
+    const float sq = b * b - 4 * a * c;
+    if (sq < __uint_as_float(0x368637bdu) * a) return float(step_out_f64(dx, dy, dz, r, jx, jy, jz));  // 4e-6
+  }
+  return step_out(dx, dy, dz, r, a, jx, jy, jz);
+}
+
 // Kahan-compensated accumulation.
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float term) {
   const float yk = term - comp;

@@ -42,6 +42,7 @@ struct ScanOut {
 // cell are ordered by structure id: the pass ends at the first entry of a
 // structure above L (the reference skips those spheres, :805-806).  Entries
 // are read kScanBatch at a time so that several loads are in flight per thread.
+template <bool T64>
 __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const int* __restrict__ sid, int start,
                                           int count, int nstructures, float x, float y, float z, int L, float a,
                                           float jx, float jy, float jz, float reach, ScanOut& o) {
@@ -95,10 +96,10 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
       const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
       if (in_mask & (1u << i)) {
         o.any_in = true;
-        const float f = step_in(dx, dy, dz, c.w, a, jx, jy, jz);
+        const float f = step_in_t<T64>(dx, dy, dz, c.w, a, jx, jy, jz);
         if (o.fin < f) o.fin = f;
       } else {
-        const float f = step_out(dx, dy, dz, c.w, a, jx, jy, jz);
+        const float f = step_out_t<T64>(dx, dy, dz, c.w, a, jx, jy, jz);
         if (f < o.fout) o.fout = f;
       }
     }
@@ -199,7 +200,8 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     const int start = __ldg((near ? J.near_start : J.cell_start) + cell);
     const int count = __ldg((near ? J.near_count : J.cell_count) + cell);
     ScanOut r;
-    if (!scan_cell(sph4, sidv, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r)) {
+    constexpr bool kT64 = (MODE & NZ_MODE_TANGENT64) != 0;
+    if (!scan_cell<kT64>(sph4, sidv, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r)) {
       label = label_of(sph4, sidv, start, count, J.nstructures, x, y, z);
       if (niter == 1) {  // the first draw's length depends on the label
         ds = sqrtf(2 * __ldg(J.D + label) * dt);
@@ -209,7 +211,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
       }
       // the full list: the near one was chosen for the old reach
       const int fs = __ldg(J.cell_start + cell), fc = __ldg(J.cell_count + cell);
-      scan_cell(J.sph4, J.sid, fs, fc, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r);
+      scan_cell<kT64>(J.sph4, J.sid, fs, fc, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r);
     }
     jc = ref_min(jc, r.any_in ? r.fin : kBig);
     jc = ref_min(jc, r.fout);
@@ -456,7 +458,14 @@ void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items,
 // jobs == null: the single job `single` with n_items CTAs of kFusedThreads walkers.
 int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
                  int step1, int* queue, int grid, int threads, cudaStream_t st) {
-  switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS)) {
+  switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS | NZ_MODE_TANGENT64)) {
+    case NZ_MODE_PHI | NZ_MODE_TANGENT64:
+      launch_mode<NZ_MODE_PHI | NZ_MODE_TANGENT64>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
+      break;
+    case NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_TANGENT64:
+      launch_mode<NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_TANGENT64>(single, jobs, items, n_items, step0, step1, queue, grid,
+                                                                 threads, st);
+      break;
     case NZ_MODE_PHI: launch_mode<NZ_MODE_PHI>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     case NZ_MODE_SIG: launch_mode<NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     case NZ_MODE_PHI | NZ_MODE_SIG:

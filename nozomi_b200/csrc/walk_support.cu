@@ -11,9 +11,9 @@ namespace nz {
 // kernel and bounded.  The label of a point is found from its cell's list:
 // every sphere that contains a point of a cell is a member of that cell.
 // ---------------------------------------------------------------------------
-__global__ void seed_kernel(nz_substrate sub, const uint8_t* __restrict__ target, int N, uint32_t k0, uint32_t k1,
-                            uint32_t stream, int max_rounds, float* __restrict__ spins, int* __restrict__ label,
-                            int* __restrict__ n_unseeded) {
+__global__ void seed_kernel(nz_substrate sub, const uint8_t* __restrict__ target, uint32_t id0, int N, uint32_t k0,
+                            uint32_t k1, uint32_t stream, int max_rounds, float* __restrict__ spins,
+                            int* __restrict__ label, int* __restrict__ n_unseeded) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= N) return;
   const Grid g{sub.grid.Lx, sub.grid.Ly, sub.grid.Lz, sub.grid.dLx, sub.grid.dLy, sub.grid.dLz,
@@ -25,7 +25,7 @@ __global__ void seed_kernel(nz_substrate sub, const uint8_t* __restrict__ target
   const int ns = sub.nstructures;
   for (int round = 0; round < max_rounds; ++round) {
     float u0, u1, u2;
-    philox_uniform3(k0, k1, stream, uint32_t(w), uint32_t(round), u0, u1, u2);
+    philox_uniform3(k0, k1, stream, id0 + uint32_t(w), uint32_t(round), u0, u1, u2);
     const float px = (u0 - 0.5f) * g.Lx;
     const float py = (u1 - 0.5f) * g.Ly;
     const float pz = (u2 - 0.5f) * g.Lz;
@@ -205,17 +205,23 @@ __global__ void __launch_bounds__(256) moments_kernel(const float* __restrict__ 
 
 using namespace nz;
 
-extern "C" int nz_seed(const nz_substrate* sub, const uint8_t* target, int N, uint32_t key0, uint32_t key1,
-                       uint32_t stream_id, int max_rounds, float* spins, int* label, int* n_unseeded, void* stream) {
+extern "C" int nz_seed_range(const nz_substrate* sub, const uint8_t* target, uint32_t id0, int N, uint32_t key0,
+                             uint32_t key1, uint32_t stream_id, int max_rounds, float* spins, int* label,
+                             int* n_unseeded, void* stream) {
   if (!sub || !target || N < 0 || max_rounds <= 0 || !spins || !n_unseeded || !sub->cell_start || !sub->cell_count ||
-      !sub->cell_items || (sub->S > 0 && !sub->spheres))
-    return set_error(NZ_ERR_ARG, "nz_seed: bad arguments");
+      !sub->cell_items || (sub->S > 0 && !sub->spheres) || uint64_t(id0) + uint64_t(N) > (uint64_t(1) << 32))
+    return set_error(NZ_ERR_ARG, "nz_seed_range: bad arguments");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(n_unseeded, 0, sizeof(int), st) != cudaSuccess) return check_launch("nz_seed memset");
   if (N == 0) return NZ_OK;
-  seed_kernel<<<(N + 255) / 256, 256, 0, st>>>(*sub, target, N, key0, key1, stream_id, max_rounds, spins, label,
-                                                n_unseeded);
+  seed_kernel<<<(N + 255) / 256, 256, 0, st>>>(*sub, target, id0, N, key0, key1, stream_id, max_rounds, spins,
+                                                label, n_unseeded);
   return check_launch("seed_kernel");
+}
+
+extern "C" int nz_seed(const nz_substrate* sub, const uint8_t* target, int N, uint32_t key0, uint32_t key1,
+                       uint32_t stream_id, int max_rounds, float* spins, int* label, int* n_unseeded, void* stream) {
+  return nz_seed_range(sub, target, 0, N, key0, key1, stream_id, max_rounds, spins, label, n_unseeded, stream);
 }
 
 static inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }

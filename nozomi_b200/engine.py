@@ -184,9 +184,10 @@ def injected_draws(table: torch.Tensor) -> L.Draws:
     return L.Draws(table.data_ptr(), int(table.shape[1]), int(table.shape[2]), 0, 0, 0)
 
 
-def seed(sub: DeviceSubstrate, targets, N: int, key: int, max_rounds: int = 100000, stream_id: int = 1):
-    """Seed N walkers uniformly into the target structures (the box is
-    structure sub.nstructures).  Returns (spins [3,N] float32, label [N])."""
+def seed(sub: DeviceSubstrate, targets, N: int, key: int, max_rounds: int = 100000, stream_id: int = 1,
+         id0: int = 0):
+    """Seed walkers [id0, id0 + N) uniformly into the target structures (the
+    box is structure sub.nstructures).  Returns (spins [3,N] float32, label [N])."""
     dev = _dev()
     tgt = np.zeros(sub.nstructures + 1, np.uint8)
     tgt[np.asarray(list(targets), np.int64)] = 1
@@ -196,8 +197,8 @@ def seed(sub: DeviceSubstrate, targets, N: int, key: int, max_rounds: int = 1000
     left = torch.zeros(1, dtype=torch.int32, device=dev)
     s = sub.struct()
     key = int(key) & 0xFFFFFFFFFFFFFFFF
-    L.check(L.load().nz_seed(L.byref(s), _p(tgt_d), N, key & 0xFFFFFFFF, key >> 32, stream_id, max_rounds, _p(spins),
-                             _p(label), _p(left), _stream()), "nz_seed")
+    L.check(L.load().nz_seed_range(L.byref(s), _p(tgt_d), int(id0), N, key & 0xFFFFFFFF, key >> 32, stream_id,
+                                   max_rounds, _p(spins), _p(label), _p(left), _stream()), "nz_seed_range")
     n_left = int(left.item())
     if n_left:
         raise NozomiError(f"seeding left {n_left} of {N} walkers unplaced after {max_rounds} rounds "

@@ -48,8 +48,9 @@ class DwiRun:
     in the gradient: phi(a) = a * phi(1))."""
 
     def __init__(self, dsub: engine.DeviceSubstrate, gwave, dirs: np.ndarray, amplitudes, N: int, seed: int = 0,
-                 targets=None, tuning: Tuning | None = None, positions: torch.Tensor | None = None):
+                 targets=None, tuning: Tuning | None = None, positions: torch.Tensor | None = None, id0: int = 0):
         self.sub = dsub
+        self.id0 = int(id0)  # global id of walker 0: a shard walks walkers [id0, id0 + N) of a larger run
         self.tuning = tuning or Tuning()
         self.dt = float(gwave.dt)
         G, Ga = step_tables(gwave)
@@ -74,7 +75,7 @@ class DwiRun:
         """(positions [3,N], labels [N]) — given, or seeded on the device."""
         if self.positions is not None:
             return self.positions, None
-        return engine.seed(self.sub, self.targets, self.N, key=self.seed ^ 0x5EED)
+        return engine.seed(self.sub, self.targets, self.N, key=self.seed ^ 0x5EED, id0=self.id0)
 
     def prepare(self, positions: torch.Tensor | None = None, labels: torch.Tensor | None = None):
         if positions is None:
@@ -83,7 +84,10 @@ class DwiRun:
         N = x.shape[1]
         lab = labels if labels is not None else torch.full((N,), -1, dtype=torch.int32, device=x.device)
         wk = engine.Walkers(x, x.clone(), phi=torch.zeros((6, N), device=x.device), label=lab)
-        self.state = engine.FusedState.from_walkers(wk)
+        ids = None
+        if self.id0:
+            ids = torch.arange(self.id0, self.id0 + N, dtype=torch.int64, device=x.device).to(torch.int32)
+        self.state = engine.FusedState.from_walkers(wk, ids)
         self.spare = engine.FusedState(N)
         self.launches = 1
         return self
@@ -124,11 +128,25 @@ class DwiRun:
         Phi [6,N], label, flags)."""
         N = self.state.N
         dev = self.state.pos.device
-        wk = engine.Walkers(torch.empty((3, N), device=dev), torch.empty((3, N), device=dev),
-                            phi=torch.empty((6, N), device=dev), label=torch.empty(N, dtype=torch.int32, device=dev),
-                            flags=torch.empty(N, dtype=torch.int32, device=dev))
-        self.state.to_walkers_by_id(wk)
-        return wk
+
+        def fresh():
+            return engine.Walkers(torch.empty((3, N), device=dev), torch.empty((3, N), device=dev),
+                                  phi=torch.empty((6, N), device=dev),
+                                  label=torch.empty(N, dtype=torch.int32, device=dev),
+                                  flags=torch.empty(N, dtype=torch.int32, device=dev))
+        wk = fresh()
+        if not self.id0:
+            self.state.to_walkers_by_id(wk)
+            return wk
+        # a shard: state order, then scattered to slot (walker id - id0)
+        self.state.to_walkers(wk)
+        slot = self.state.walker_ids().to(torch.int64) - self.id0
+        out = fresh()
+        for name in ("spins", "spins0", "phi"):
+            getattr(out, name)[:, slot] = getattr(wk, name)
+        for name in ("label", "flags"):
+            getattr(out, name)[slot] = getattr(wk, name)
+        return out
 
     def phase(self) -> torch.Tensor:
         """Per-walker phase [ndir, N] of the unit waveform, walker-id order."""

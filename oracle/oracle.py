@@ -30,7 +30,8 @@ class _Geom(ctypes.Structure):
 
 class _Rng(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("normals", _P), ("nsteps", ctypes.c_int), ("maxk", ctypes.c_int),
-                ("key0", ctypes.c_uint32), ("key1", ctypes.c_uint32), ("stream", ctypes.c_uint32)]
+                ("key0", ctypes.c_uint32), ("key1", ctypes.c_uint32), ("stream", ctypes.c_uint32),
+                ("id0", ctypes.c_uint32)]
 
 
 _lib = None
@@ -44,6 +45,7 @@ def lib():
         _lib.oz_walk_f32.argtypes = [_P, _P, i, i, i, i, f, _P, _P, _P, _P, _P, _P, i, _P, _P, _P, _P, _P, _P, _P, i]
         _lib.oz_walk_f64.argtypes = [_P, _P, i, i, i, i, d, _P, _P, _P, _P, _P, _P, i, _P, _P, _P, _P, _P, _P, i]
         _lib.oz_seed.argtypes = [_P, _P, i, u, u, u, i, _P, _P, i]
+        _lib.oz_seed_range.argtypes = [_P, _P, u, i, u, u, u, i, _P, _P, i]
         _lib.oz_seed_accept.argtypes = [_P, _P, i, _P, _P]
         _lib.oz_philox_normals.argtypes = [u, u, u, i, i, i, _P]
         _lib.oz_moments.argtypes = [i, _P, _P, _P]
@@ -51,7 +53,9 @@ def lib():
         _lib.oz_signal_phase.argtypes = [i, _P, i, _P, i, _P, _P]
         _lib.oz_cells.argtypes = [_P, i, d, d, d, i, i, i, d, _P, _P, _P]
         _lib.oz_cells.restype = ctypes.c_longlong
-        for fn in ("oz_walk_f32", "oz_walk_f64", "oz_seed"):
+        _lib.oz_set_phase64.argtypes = [_P]
+        _lib.oz_set_phase64.restype = None
+        for fn in ("oz_walk_f32", "oz_walk_f64", "oz_seed", "oz_seed_range"):
             getattr(_lib, fn).restype = ctypes.c_int
         for fn in ("oz_seed_accept", "oz_philox_normals", "oz_moments", "oz_signal_phi", "oz_signal_phase"):
             getattr(_lib, fn).restype = None
@@ -118,20 +122,24 @@ class Geometry:
 
 def injected(normals: np.ndarray):
     n = np.ascontiguousarray(normals, dtype=np.float32)
-    r = _Rng(RNG_INJECT, n.ctypes.data, n.shape[1], n.shape[2], 0, 0, 0)
+    r = _Rng(RNG_INJECT, n.ctypes.data, n.shape[1], n.shape[2], 0, 0, 0, 0)
     r._keep = n
     return r
 
 
-def philox(key0: int, key1: int = 0, stream: int = 0):
-    return _Rng(RNG_PHILOX, None, 0, 0, key0 & 0xFFFFFFFF, key1 & 0xFFFFFFFF, stream & 0xFFFFFFFF)
+def philox(key0: int, key1: int = 0, stream: int = 0, id0: int = 0):
+    """Philox draws; walker w of the call draws as global walker id0 + w."""
+    return _Rng(RNG_PHILOX, None, 0, 0, key0 & 0xFFFFFFFF, key1 & 0xFFFFFFFF, stream & 0xFFFFFFFF,
+                id0 & 0xFFFFFFFF)
 
 
 def walk_f32(geom: Geometry, rng, mode: int, spins, spins0, step0: int, nsteps: int, dt: float,
              G=None, Garea=None, phase=None, diffdir=None, sig=None, phi=None,
-             counters: bool = True, work: bool = False, nthreads: int = 0):
+             counters: bool = True, work: bool = False, nthreads: int = 0, phase64=None):
     """Run steps [step0, step0+nsteps) in place on float32 arrays.  Returns a
-    dict of per-walker label / n_iter / n_scatter / flags (and work sums)."""
+    dict of per-walker label / n_iter / n_scatter / flags (and work sums).
+    phase64: optional [ndir, N] float64 receiving the exact (FP64) phase of
+    this single-precision trajectory along diffdir."""
     N = spins.shape[1]
     g = geom.struct()
     lab = np.zeros(N, np.int32) if counters else None
@@ -143,10 +151,14 @@ def walk_f32(geom: Geometry, rng, mode: int, spins, spins0, step0: int, nsteps: 
     Garea = None if Garea is None else np.ascontiguousarray(Garea, np.float32)
     dd = None if diffdir is None else np.ascontiguousarray(diffdir, np.float32)
     ndir = 0 if dd is None else dd.shape[1]
-    rc = lib().oz_walk_f32(ctypes.byref(g), ctypes.byref(rng), mode, N, step0, nsteps, float(dt),
-                           _ptr(G), _ptr(Garea), _ptr(spins), _ptr(spins0), _ptr(phase), _ptr(dd), ndir,
-                           _ptr(sig), _ptr(phi), _ptr(lab), _ptr(nit), _ptr(nsc), _ptr(flg), _ptr(wk),
-                           nthreads)
+    lib().oz_set_phase64(_ptr(phase64))
+    try:
+        rc = lib().oz_walk_f32(ctypes.byref(g), ctypes.byref(rng), mode, N, step0, nsteps, float(dt),
+                               _ptr(G), _ptr(Garea), _ptr(spins), _ptr(spins0), _ptr(phase), _ptr(dd), ndir,
+                               _ptr(sig), _ptr(phi), _ptr(lab), _ptr(nit), _ptr(nsc), _ptr(flg), _ptr(wk),
+                               nthreads)
+    finally:
+        lib().oz_set_phase64(None)
     if rc != 0:
         raise RuntimeError(f"oz_walk_f32 failed ({rc})")
     return {"label": lab, "n_iter": nit, "n_scatter": nsc, "flags": flg, "work": wk}
@@ -173,14 +185,16 @@ def walk_f64(geom: Geometry, rng, mode: int, spins, spins0, step0: int, nsteps: 
 
 
 def seed(geom: Geometry, targets, N: int, key0: int, key1: int = 0, stream: int = 1,
-         max_rounds: int = 10000, nthreads: int = 0):
+         max_rounds: int = 10000, nthreads: int = 0, id0: int = 0):
+    """Seed walkers [id0, id0 + N) (oz_seed_range); returns (spins, label, left)."""
     tgt = np.zeros(geom.nstructures + 1, np.uint8)
     tgt[np.asarray(list(targets), dtype=np.int64)] = 1
     spins = np.full((3, N), np.nan, np.float32)
     label = np.zeros(N, np.int32)
     g = geom.struct()
-    left = lib().oz_seed(ctypes.byref(g), tgt.ctypes.data, N, key0 & 0xFFFFFFFF, key1 & 0xFFFFFFFF,
-                         stream, max_rounds, spins.ctypes.data, label.ctypes.data, nthreads)
+    left = lib().oz_seed_range(ctypes.byref(g), tgt.ctypes.data, id0 & 0xFFFFFFFF, N, key0 & 0xFFFFFFFF,
+                               key1 & 0xFFFFFFFF, stream, max_rounds, spins.ctypes.data, label.ctypes.data,
+                               nthreads)
     return spins, label, left
 
 

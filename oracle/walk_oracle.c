@@ -70,12 +70,13 @@ typedef struct oz_rng {
     const float* normals;   /* injected: [N][nsteps][maxk], k-th normal of a walker's step */
     int nsteps, maxk;
     uint32_t key0, key1, stream;
+    uint32_t id0;           /* Philox: walker w draws at counter id0 + w (a shard's first global id) */
 } oz_rng;
 
 static inline void oz_draw3(const oz_rng* rng, int w, int step, int draw,
                             float* n0, float* n1, float* n2, int* flags) {
     if (rng->kind == OZ_RNG_PHILOX) {
-        oz_philox_normal3(rng->key0, rng->key1, rng->stream, (uint32_t)w, (uint32_t)step,
+        oz_philox_normal3(rng->key0, rng->key1, rng->stream, rng->id0 + (uint32_t)w, (uint32_t)step,
                           (uint32_t)draw, n0, n1, n2);
         return;
     }
@@ -124,6 +125,10 @@ static double oz_out_tol_f64(double dx, double dy, double dz, double r, double j
     else if ((fpos < 0 && fneg < 0) || (b > 0)) return 1e6;
     return 0;
 }
+
+/* Optional FP64 phase of the single-precision trajectory ([ndir, N], set by
+ * oz_set_phase64 for the next oz_walk_f32 call; needs diffdir). */
+static double* g_phase64 = NULL;
 
 /* ---- single precision, the reference's arithmetic ---- */
 #define REAL float
@@ -181,12 +186,14 @@ OZ_API int oz_walk_f32(const oz_geom* g, const oz_rng* rng, int mode, int N, int
         for (int s = step0; s < step0 + nsteps; ++s)
             oz_walker_step_f32(g, rng, mode, N, w, s, dt, G ? G[s] : 0.0f, Garea ? Garea[s] : 0.0f,
                                spins, spins0, phase, diffdir, ndir, sig, phi, label, n_iter, n_scatter,
-                               flags, work ? wk : NULL);
+                               flags, work ? wk : NULL, g_phase64);
         acc0 += wk[0]; acc1 += wk[1]; acc2 += wk[2];
     }
     if (work) { work[0] += acc0; work[1] += acc1; work[2] += acc2; }
     return 0;
 }
+
+OZ_API void oz_set_phase64(double* phase64) { g_phase64 = phase64; }
 
 OZ_API int oz_walk_f64(const oz_geom* g, const oz_rng* rng, int mode, int N, int step0, int nsteps,
                        double dt, const double* G, const double* Garea,
@@ -200,7 +207,7 @@ OZ_API int oz_walk_f64(const oz_geom* g, const oz_rng* rng, int mode, int N, int
         for (int s = step0; s < step0 + nsteps; ++s)
             oz_walker_step_f64(g, rng, mode, N, w, s, dt, G ? G[s] : 0.0, Garea ? Garea[s] : 0.0,
                                spins, spins0, phase, diffdir, ndir, sig, phi, label, n_iter, n_scatter,
-                               flags, NULL);
+                               flags, NULL, NULL);
     return 0;
 }
 
@@ -234,8 +241,8 @@ static int oz_label_of(const oz_geom* g, float px, float py, float pz) {
  * (walker, r, 0, stream); at most max_rounds rounds.  Returns the number of
  * walkers left unseeded.
  */
-OZ_API int oz_seed(const oz_geom* g, const unsigned char* target, int N, uint32_t key0, uint32_t key1,
-                   uint32_t stream, int max_rounds, float* spins, int* label, int nthreads) {
+OZ_API int oz_seed_range(const oz_geom* g, const unsigned char* target, uint32_t id0, int N, uint32_t key0,
+                         uint32_t key1, uint32_t stream, int max_rounds, float* spins, int* label, int nthreads) {
     const int nt = oz_threads(nthreads);
     int unseeded = 0;
 #pragma omp parallel for num_threads(nt) schedule(dynamic, 256) reduction(+:unseeded)
@@ -243,7 +250,7 @@ OZ_API int oz_seed(const oz_geom* g, const unsigned char* target, int N, uint32_
         int ok = 0;
         for (int r = 0; r < max_rounds && !ok; ++r) {
             float u0, u1, u2;
-            oz_philox_uniform3(key0, key1, stream, (uint32_t)w, (uint32_t)r, &u0, &u1, &u2);
+            oz_philox_uniform3(key0, key1, stream, id0 + (uint32_t)w, (uint32_t)r, &u0, &u1, &u2);
             float px = (u0 - 0.5f) * g->Lx;
             float py = (u1 - 0.5f) * g->Ly;
             float pz = (u2 - 0.5f) * g->Lz;
@@ -265,6 +272,13 @@ OZ_API int oz_seed(const oz_geom* g, const unsigned char* target, int N, uint32_
         }
     }
     return unseeded;
+}
+
+/* Walkers [id0, id0 + N) of the same seeding: walker id0 + w lands in slot w,
+ * so shards of a run seed exactly the walkers of the unsharded run. */
+OZ_API int oz_seed(const oz_geom* g, const unsigned char* target, int N, uint32_t key0, uint32_t key1,
+                   uint32_t stream, int max_rounds, float* spins, int* label, int nthreads) {
+    return oz_seed_range(g, target, 0, N, key0, key1, stream, max_rounds, spins, label, nthreads);
 }
 
 /* Accept/reject of given positions under the seeding rule (pinned against the

@@ -99,3 +99,17 @@ def test_batch_graph_replay_is_repeatable(batch_result):
         torch.cuda.synchronize()
         for s, ref in zip(b.signals(), sig):
             np.testing.assert_allclose(s, ref, rtol=0, atol=1e-12)
+
+
+def test_autotune_small(tmp_path):
+    from nozomi_b200.autotune import autotune
+    specs = _specs()
+    space = {"threads": [64, 128], "cell": [1.0], "near_margin": [0.5, None], "steps_per_launch": [100, 200],
+             "coarsen": [4]}
+    cache_file = tmp_path / "tune.json"
+    t, threads, rep = autotune(specs, space=space, trial_steps=200, max_walkers=2000, max_jobs=2,
+                               cache_file=cache_file)
+    assert threads in (64, 128) and t.steps_per_launch in (100, 200) and not rep["cached"]
+    assert len(rep["trials"]) >= 3
+    t2, threads2, rep2 = autotune(specs, space=space, cache_file=cache_file)
+    assert rep2["cached"] and threads2 == threads and t2 == t
