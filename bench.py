@@ -13,10 +13,13 @@ weak scaling, no data-path collective).  `e2e` is the same metric through the
 public call with host buffers: positions copied in from pinned memory and the
 signal copied out every step.
 
---impl reference: the reference has no CPU implementation of the walk, so the
-reference arm times the oracle (a C/OpenMP restatement of the reference kernel,
-oracle/walk_oracle.c) on the host cores, on a bounded sample of the same
-workload.
+--impl reference: the reference has no CPU implementation of the walk; the
+reference arm times the reference's own kernel source compiled for the CPU
+(oracle/_ref, built where the reference tree is present: its launches run as
+OpenMP loops over walkers on the host cores) on a bounded sample of the same
+workload, or, without that build, the oracle's C restatement of the kernel.
+--impl reference_gpu: the reference's kernel compiled for sm_100a (baseline/_ref)
+launched on this GPU one waveform sample at a time, as the reference does.
 """
 from __future__ import annotations
 
@@ -44,7 +47,11 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference_gpu"],
+                    help="reference: the reference's walk on the host cores; reference_gpu: the reference's own "
+                         "CUDA kernel (baseline/_ref build) on this GPU, one launch per waveform sample")
+    ap.add_argument("--ref-samples", type=int, default=600,
+                    help="reference_gpu: waveform samples (launches) timed, after --warmup x 10 untimed")
     ap.add_argument("--walkers", type=int, default=1_000_000)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the CPU baseline sample")
@@ -69,15 +76,8 @@ def parse():
 
 
 def workload():
-    from nozomi_b200 import substrates as sb
-    from nozomi_b200.waveforms import PGDiffWaveform
-    sub = sb.packed_axons(seed=2)
-    pg = PGDiffWaveform(20.0, 10.0, 30.0, time_step=0.005)
-    rng = np.random.default_rng(2)
-    dirs = rng.standard_normal((3, 30))
-    dirs /= np.linalg.norm(dirs, axis=0)
-    bvals = np.array([0.0, 1.0, 2.0, 3.0])
-    return sub, pg, dirs, bvals
+    from nozomi_b200.workloads import packed_workload
+    return packed_workload()
 
 
 # ---------------------------------------------------------------------------
@@ -127,6 +127,88 @@ def cpu_sample(sub, pg, dirs, cell, seconds, rank_seed=0, work=True):
     return value, cores, sample, wk
 
 
+REF_CPU_BUILD = "packed_cpu_16k"
+REF_CPU_KIND = ("the reference's own sim3d_kernel.cu (randomWalk3d_phase_multidirr, template filled as DiffSim3d "
+                "does, padded set_segments table at 1 um cells) compiled for the CPU with host stand-ins for its "
+                "CUDA headers (oracle/refshim): each kernel launch runs its 1000-thread blocks as OpenMP "
+                "iterations over walkers; curand_normal reads the oracle's Philox normals")
+
+
+class ReferenceCpu:
+    """The reference kernel's CPU build (oracle/_ref, named build) walking
+    the first N walkers of the packed workload, launch by launch."""
+
+    def __init__(self, sub, pg, dirs, key=1000):
+        import ctypes
+        from oracle import oracle as oz
+        from oracle.build import reference_named
+        b = reference_named(REF_CPU_BUILD)
+        if b is None:
+            raise FileNotFoundError(f"oracle/_ref build {REF_CPU_BUILD} is absent")
+        so, pars = b
+        self.lib = ctypes.CDLL(str(so))
+        P, f, i = ctypes.c_void_p, ctypes.c_float, ctypes.c_int
+        self.lib.ref_run_walk_multidir.argtypes = [i, i, i, f, P, P, P, P, P, f, f, P, i]
+        self.lib.ref_run_initstates.argtypes = [i, i, i]
+        self.lib.ref_set_philox.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint]
+        from nozomi_b200.substrates import cell_grid
+        from nozomi_b200.waveforms import step_tables
+        self.N = N = int(pars["nspins"])
+        nseg = cell_grid(sub.L, 1.0)
+        if (int(pars["nLx"]), int(pars["nLy"]), int(pars["nLz"])) != tuple(nseg) or int(pars["nspheres"]) != sub.S:
+            raise ValueError("the reference CPU build does not match this workload")
+        sph64 = sub.spheres()
+        st, ct, it = oz.cells(sph64, sub.L, nseg)
+        self.K = K = int(pars["nspheres_per_seg"])
+        if int(ct.max()) != K:
+            raise ValueError(f"cell table K={int(ct.max())} but the build has {K}")
+        self.seg = oz.segments(sph64, sub.L, nseg, K)
+        ns = sub.nstructures
+        g = oz.Geometry(sph64.astype(np.float32), ns, sub.L, nseg, st, ct, it, np.full(ns + 1, 2.0, np.float32),
+                        np.full(ns + 1, 100.0, np.float32))
+        x, _, left = oz.seed(g, list(range(ns + 1)), N, key ^ 0x5EED)
+        self.spins = np.ascontiguousarray(x.reshape(-1))
+        self.spins0 = self.spins.copy()
+        self.ndir = dirs.shape[1]
+        self.phase = np.zeros(self.ndir * N, np.float32)
+        self.sph = np.ascontiguousarray(sph64.astype(np.float32))
+        self.dd = np.ascontiguousarray(dirs.astype(np.float32))
+        self.G, self.Ga = step_tables(pg)
+        self.dt = float(pg.dt)
+        self.lib.ref_run_initstates(N // 1000, 1000, 1000)
+        self.lib.ref_set_philox(key, 0, 0)
+        self.n = 0
+
+    def run(self, nsteps):
+        """Launch the next nsteps waveform samples (wrapping to the start)."""
+        f = float
+        for _ in range(nsteps):
+            n = self.n % self.G.size
+            self.lib.ref_run_walk_multidir(self.N // 1000, 1000, n, f(self.dt), self.sph.ctypes.data,
+                                           self.seg.ctypes.data, self.spins.ctypes.data, self.spins0.ctypes.data,
+                                           self.phase.ctypes.data, f(self.G[n]), f(self.Ga[n]), self.dd.ctypes.data,
+                                           self.ndir)
+            self.n += 1
+
+
+def reference_cpu_sample(sub, pg, dirs, seconds, steps=1, warmup=0):
+    """Time the reference kernel's CPU build: `warmup` + `steps` samples of
+    about `seconds` each.  Returns (walker-steps/s, cores, sample text)."""
+    cores = os.cpu_count() or 1
+    r = ReferenceCpu(sub, pg, dirs)
+    t = time.perf_counter()
+    r.run(5)
+    rate = r.N * 5 / (time.perf_counter() - t)
+    per = int(np.clip(seconds * rate / r.N, 5, r.G.size))
+    r.run(per * warmup)
+    t = time.perf_counter()
+    r.run(per * steps)
+    el = time.perf_counter() - t
+    sample = (f"{r.N} walkers x {per} launches per step x {steps} step(s) (waveform samples "
+              f"{5 + per * warmup}..{5 + per * (warmup + steps) - 1}), {el:.1f} s, padded K={r.K}")
+    return r.N * per * steps / el, cores, sample
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -134,23 +216,26 @@ def run_reference(args):
     sub, pg, dirs, bvals = workload()
     from oracle.build import build_oracle
     build_oracle()
-    total_t, total_ws = 0.0, 0
-    value = cores = sample = None
-    for i in range(args.warmup + args.steps):
-        v, cores, sample, _ = cpu_sample(sub, pg, dirs, args.cell or 1.0, args.cpu_seconds / 2, rank_seed=i,
-                                         work=False)
-        if i >= args.warmup:
-            total_ws += 1
-            total_t += 1.0 / v
-            value = v if value is None else value
-    value = total_ws / total_t
+    try:
+        value, cores, sample = reference_cpu_sample(sub, pg, dirs, args.cpu_seconds / 2, steps=args.steps,
+                                                    warmup=args.warmup)
+        kind, how = "reference", REF_CPU_KIND
+    except (FileNotFoundError, ValueError) as e:  # no reference build on this host: the C restatement
+        total_t, total_ws = 0.0, 0
+        for i in range(args.warmup + args.steps):
+            v, cores, sample, _ = cpu_sample(sub, pg, dirs, args.cell or 1.0, args.cpu_seconds / 2, rank_seed=i,
+                                             work=False)
+            if i >= args.warmup:
+                total_ws += 1
+                total_t += 1.0 / v
+        value = total_ws / total_t
+        kind, how = "port", f"oracle/walk_oracle.c, the C restatement of the kernel, OpenMP over walkers ({e})"
     line = {"impl": "reference", "metric": "walker-steps/s", "value": value, "unit": "walker-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cell_um": args.cell or 1.0},
-            "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": "port",
-                             "sample": sample + "; oracle/walk_oracle.c (C restatement of sim3d_kernel.cu's "
-                                                "walk, OpenMP over walkers)"},
+            "config": {"workload": WORKLOAD, "cell_um": 1.0},
+            "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": kind,
+                             "sample": sample + "; " + how},
             "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -351,9 +436,15 @@ def run_ours(args):
         cpu = None
         wk = None
         if world == 1 and not args.no_cpu_baseline:
-            v, cores, sample, wk = cpu_sample(sub, pg, dirs, tuning.cell, args.cpu_seconds)
-            cpu = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "port",
-                   "sample": sample + "; oracle/walk_oracle.c, OpenMP over walkers"}
+            v, cores, sample, wk = cpu_sample(sub, pg, dirs, tuning.cell, args.cpu_seconds / 2)
+            port = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "port",
+                    "sample": sample + "; oracle/walk_oracle.c, OpenMP over walkers"}
+            try:
+                v, cores, sample = reference_cpu_sample(sub, pg, dirs, args.cpu_seconds / 2)
+                cpu = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "reference",
+                       "sample": sample + "; " + REF_CPU_KIND, "port": port}
+            except (FileNotFoundError, ValueError) as e:
+                cpu = dict(port, reference_unavailable=str(e))
         peaks = {}
         pk = ROOT / "MEASURED_PEAKS.json"
         if pk.exists():
@@ -565,10 +656,72 @@ def run_serving(args):
     return 0
 
 
+def run_reference_gpu(args):
+    """The reference's own kernel, randomWalk3d_phase_multidirr, compiled from
+    its source with its %-template filled in for this workload (baseline/_ref,
+    built where the reference tree is present) and launched as
+    DwiSim3d.simulate_multi_directions does: block 1000, one launch per
+    waveform sample, cuRAND XORWOW draws, the padded cell table of
+    set_segments.  The walkers are the ones the fused arm seeds.  Times
+    --ref-samples launches; walker-steps/s = walkers x launches / time."""
+    import torch
+    from baseline.reference_gpu import RefGpuWalk
+    from nozomi_b200 import engine
+    from nozomi_b200.simulate import device_substrate
+    from nozomi_b200.waveforms import step_tables
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    engine.require_cuda()
+    sub, pg, dirs, bvals = workload()
+    ref = RefGpuWalk("packed_1e6")
+    N = ref.N
+    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=1.0)
+    K, seg = dsub.padded_segments()
+    x0, _ = engine.seed(dsub, list(range(sub.nstructures + 1)), N, key=1000 ^ 0x5EED)
+    sph = torch.from_numpy(sub.spheres().astype(np.float32)).cuda()
+    dd = torch.from_numpy(dirs.astype(np.float32)).cuda()
+    ref.setup(sph, seg, K, x0, dirs.shape[1], dd)
+    ref.initstates(1000)
+    G, Ga = step_tables(pg)
+    dt = np.float32(pg.dt)
+    nwarm = max(3, args.warmup) * 10
+    for n in range(nwarm):
+        ref.step(dt, G[n], Ga[n])
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n1 = min(G.size, nwarm + args.ref_samples)
+    e0.record(stream)
+    for n in range(nwarm, n1):
+        ref.step(dt, G[n], Ga[n])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = n1 - nwarm
+    value = N * launches / (ms * 1e-3)
+    line = {"impl": "reference_gpu", "metric": "walker-steps/s", "value": value, "unit": "walker-steps/s",
+            "n_gpus": 1, "steps": launches, "warmup": nwarm, "ms_per_step": ms / launches,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded packed-axon substrate, seeded walkers)",
+            "config": {"workload": WORKLOAD, "walkers": N, "cell_um": 1.0, "padded_cell_table_K": K,
+                       "samples_timed": f"waveform samples {nwarm}..{n1 - 1} of {G.size}",
+                       "kernel": "randomWalk3d_phase_multidirr (sim3d_kernel.cu:719-943), block 1000, "
+                                 "one launch per sample"},
+            "gpu_launches": launches, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.impl == "reference_gpu":
+        return run_reference_gpu(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "serving":

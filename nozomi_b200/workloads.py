@@ -32,6 +32,20 @@ CACHE = Path(os.environ.get("NOZOMI_B200_CACHE", Path.home() / ".cache" / "nozom
 DT = 0.005
 
 
+def packed_workload():
+    """The packed-substrate workload: 200 beaded axons x 100 spheres in a
+    periodic 40x40x80 um box (seed 2), PGSE 20/10/30 ms at dt = 5 us (6000
+    steps), 30 directions uniform on the sphere (seed 2), b in {0,1,2,3}
+    ms/um^2.  Returns (substrate, waveform, dirs [3,30], b-values)."""
+    from . import substrates as sb
+    sub = sb.packed_axons(seed=2)
+    pg = PGDiffWaveform(20.0, 10.0, 30.0, time_step=0.005)
+    rng = np.random.default_rng(2)
+    dirs = rng.standard_normal((3, 30))
+    dirs /= np.linalg.norm(dirs, axis=0)
+    return sub, pg, dirs, np.array([0.0, 1.0, 2.0, 3.0])
+
+
 def bundle(n_axons: int, seed: int) -> Substrate:
     CACHE.mkdir(parents=True, exist_ok=True)
     key = hashlib.sha1(f"axon_bundle-v1-{n_axons}-{seed}".encode()).hexdigest()[:16]

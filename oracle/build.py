@@ -74,5 +74,46 @@ def build_reference_kernel(code: str) -> Path:
     return so
 
 
+REF_INDEX = REF_OUT / "index.json"
+
+# named CPU builds of the reference kernel that bench.py's reference arm loads
+# on a host without the reference tree: name -> walker count of the build
+BENCH_BUILDS = {"packed_cpu_16k": 16_000}
+
+
+def build_reference_named(name: str, pars: dict) -> Path:
+    """build_reference_kernel for `pars`, recorded under `name` in
+    oracle/_ref/index.json with its pars."""
+    import json
+    so = build_reference_kernel(substitute_reference(pars))
+    idx = json.loads(REF_INDEX.read_text()) if REF_INDEX.exists() else {}
+    idx[name] = {"so": so.name, "pars": pars}
+    REF_INDEX.write_text(json.dumps(idx, indent=1))
+    return so
+
+
+def reference_named(name: str):
+    """(so path, pars) of a named CPU build of the reference kernel, or None."""
+    import json
+    if not REF_INDEX.exists():
+        return None
+    e = json.loads(REF_INDEX.read_text()).get(name)
+    if not e or not (REF_OUT / e["so"]).exists():
+        return None
+    return REF_OUT / e["so"], e["pars"]
+
+
+def build_reference_bench() -> list:
+    """The CPU builds of the reference kernel for bench.py's packed workload
+    (1 um cells; template constants as DiffSim3d forms them), where the
+    reference tree is present."""
+    if not reference_available():
+        return []
+    import sys
+    sys.path.insert(0, str(ORACLE_DIR.parent))
+    from baseline.reference_gpu import workload_pars
+    return [build_reference_named(name, workload_pars("packed_1e6", nspins=n)) for name, n in BENCH_BUILDS.items()]
+
+
 if __name__ == "__main__":
     print(build_oracle(force=True))

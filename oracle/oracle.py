@@ -46,6 +46,8 @@ def lib():
         _lib.oz_walk_f64.argtypes = [_P, _P, i, i, i, i, d, _P, _P, _P, _P, _P, _P, i, _P, _P, _P, _P, _P, _P, i]
         _lib.oz_seed.argtypes = [_P, _P, i, u, u, u, i, _P, _P, i]
         _lib.oz_seed_range.argtypes = [_P, _P, u, i, u, u, u, i, _P, _P, i]
+        _lib.oz_segments.argtypes = [_P, i, d, d, d, i, i, i, i, _P, i]
+        _lib.oz_segments.restype = ctypes.c_int
         _lib.oz_seed_accept.argtypes = [_P, _P, i, _P, _P]
         _lib.oz_philox_normals.argtypes = [u, u, u, i, i, i, _P]
         _lib.oz_moments.argtypes = [i, _P, _P, _P]
@@ -76,6 +78,18 @@ def cells(spheres64, L, nseg, jump_tol: float = 1.0):
     lib().oz_cells(sph.ctypes.data, sph.shape[1], Lx, Ly, Lz, nx, ny, nz, jump_tol, count.ctypes.data,
                    start.ctypes.data, items.ctypes.data)
     return start, count, items[:int(total)]
+
+
+def segments(spheres64, L, nseg, K: int, nthreads: int = 0):
+    """The reference's padded table [ncell*K] (oz_segments)."""
+    sph = np.ascontiguousarray(spheres64, np.float64)
+    nx, ny, nz = (int(v) for v in nseg)
+    seg = np.zeros(nx * ny * nz * int(K), np.int32)
+    rc = lib().oz_segments(sph.ctypes.data, sph.shape[1], *(float(v) for v in L), nx, ny, nz, int(K),
+                           seg.ctypes.data, nthreads)
+    if rc:
+        raise RuntimeError(f"oz_segments failed ({rc})")
+    return seg
 
 
 def _ptr(a):

@@ -408,3 +408,82 @@ OZ_API long long oz_cells(const double* sph, int S, double Lx, double Ly, double
     }
     return total;
 }
+
+/*
+ * The reference's padded cell table (diffsim3d.py:144-168): K = the largest
+ * member count; cell c = p*nx*ny + m*nx + n gets, at seg[c*K], the K spheres
+ * of smallest in_segment (ties to the lower index; numpy's unstable argsort
+ * leaves them unspecified), ascending by index.  in_segment is the maximum of
+ * six per-axis terms, so each axis's terms are computed once per (cell
+ * column, sphere) and combined per cell.
+ */
+static inline int oz_heap_less(double va, int ia, double vb, int ib) { return va < vb || (va == vb && ia < ib); }
+
+static void oz_heap_sift_down(double* hv, int* hi, int n, int i) {
+    for (;;) {
+        int l = 2*i + 1, r = l + 1, m = i;
+        if (l < n && oz_heap_less(hv[m], hi[m], hv[l], hi[l])) m = l;
+        if (r < n && oz_heap_less(hv[m], hi[m], hv[r], hi[r])) m = r;
+        if (m == i) return;
+        double tv = hv[i]; hv[i] = hv[m]; hv[m] = tv;
+        int ti = hi[i]; hi[i] = hi[m]; hi[m] = ti;
+        i = m;
+    }
+}
+
+static void oz_heap_sift_up(double* hv, int* hi, int i) {
+    while (i > 0) {
+        int p = (i - 1) / 2;
+        if (!oz_heap_less(hv[p], hi[p], hv[i], hi[i])) return;
+        double tv = hv[i]; hv[i] = hv[p]; hv[p] = tv;
+        int ti = hi[i]; hi[i] = hi[p]; hi[p] = ti;
+        i = p;
+    }
+}
+
+static int oz_cmp_int(const void* a, const void* b) { return (*(const int*)a > *(const int*)b) - (*(const int*)a < *(const int*)b); }
+
+OZ_API int oz_segments(const double* sph, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz, int K,
+                       int* seg, int nthreads) {
+    if (K <= 0 || K > S) return -1;
+    const double dLx = Lx / nx, dLy = Ly / ny, dLz = Lz / nz;
+    double* vx = (double*)malloc(sizeof(double) * (size_t)nx * S);
+    double* vy = (double*)malloc(sizeof(double) * (size_t)ny * S);
+    double* vz = (double*)malloc(sizeof(double) * (size_t)nz * S);
+    if (!vx || !vy || !vz) { free(vx); free(vy); free(vz); return -2; }
+    for (int s = 0; s < S; ++s) {
+        const double x = sph[s], y = sph[S + s], z = sph[2*S + s], r = sph[3*S + s];
+        for (int n = 0; n < nx; ++n) vx[(size_t)n*S + s] = OZ_MAX(oz_seg_lo(n, dLx, r, x, Lx), oz_seg_hi(n, dLx, r, x, Lx));
+        for (int m = 0; m < ny; ++m) vy[(size_t)m*S + s] = OZ_MAX(oz_seg_lo(m, dLy, r, y, Ly), oz_seg_hi(m, dLy, r, y, Ly));
+        for (int p = 0; p < nz; ++p) vz[(size_t)p*S + s] = OZ_MAX(oz_seg_lo(p, dLz, r, z, Lz), oz_seg_hi(p, dLz, r, z, Lz));
+    }
+    const long long ncell = (long long)nx * ny * nz;
+    const int nt = oz_threads(nthreads);
+#pragma omp parallel num_threads(nt)
+    {
+        double* hv = (double*)malloc(sizeof(double) * K);
+        int* hi = (int*)malloc(sizeof(int) * K);
+#pragma omp for schedule(dynamic, 64)
+        for (long long c = 0; c < ncell; ++c) {
+            const int n = (int)(c % nx), m = (int)((c / nx) % ny), p = (int)(c / ((long long)nx * ny));
+            const double* ax = vx + (size_t)n*S;
+            const double* ay = vy + (size_t)m*S;
+            const double* az = vz + (size_t)p*S;
+            int h = 0;
+            for (int s = 0; s < S; ++s) {
+                const double v = OZ_MAX(OZ_MAX(ax[s], ay[s]), az[s]);
+                if (h < K) {
+                    hv[h] = v; hi[h] = s; oz_heap_sift_up(hv, hi, h); ++h;
+                } else if (oz_heap_less(v, s, hv[0], hi[0])) {
+                    hv[0] = v; hi[0] = s; oz_heap_sift_down(hv, hi, K, 0);
+                }
+            }
+            int* out = seg + c * K;
+            memcpy(out, hi, sizeof(int) * K);
+            qsort(out, K, sizeof(int), oz_cmp_int);
+        }
+        free(hv); free(hi);
+    }
+    free(vx); free(vy); free(vz);
+    return 0;
+}
