@@ -4,8 +4,8 @@ Chooses walkers per CTA (``threads``), cell edge, near-list margin, steps per
 launch and re-binning coarsening by timing short trials of the batch itself:
 at most ``max_jobs`` jobs (the largest), each cut to ``max_walkers`` walkers
 and its first ``trial_steps`` steps.  The search is coordinate descent from
-the defaults, one parameter at a time, keeping a change only if it is faster
-by more than ``min_gain``.  Choices are cached per (GPU, workload signature)
+the defaults (each restricted to the search space), one parameter at a
+time, keeping a change only if it is faster by more than ``min_gain``.  Choices are cached per (GPU, workload signature)
 in a JSON file so later runs of the same shape skip the search.
 """
 from __future__ import annotations
@@ -84,7 +84,9 @@ def autotune(specs, space=None, trial_steps: int = 2000, max_walkers: int = 50_0
             return t, saved["threads"], {"cached": True, "signature": sig, **saved}
     trial = _trial_specs(specs, max_jobs, max_walkers, trial_steps)
     cache = SubstrateCache()
-    cur = {"threads": 128, "cell": 1.0, "near_margin": 0.5, "steps_per_launch": 500, "coarsen": 4}
+    # start from the defaults, or a space's first value where it lacks the default
+    default = {"threads": 128, "cell": 1.0, "near_margin": 0.5, "steps_per_launch": 500, "coarsen": 4}
+    cur = {k: (v if v in space[k] else space[k][0]) for k, v in default.items()}
     trials = []
 
     def measure(cfg):

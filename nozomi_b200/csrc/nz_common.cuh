@@ -218,6 +218,32 @@ __device__ __forceinline__ float step_out(float dx, float dy, float dz, float r,
   return 0;
 }
 
+// step_in (inside) or step_out (outside) as one instruction stream: the two
+// differ only in r -/+ tol and in how the roots are read, so lanes of a warp
+// taking different sides share the arithmetic instead of running both
+// branches.  Every operation is the one step_in / step_out performs, on the
+// same operands, so the results are theirs bit for bit.
+__device__ __forceinline__ float step_either(bool inside, float dx, float dy, float dz, float r, float a, float jx,
+                                             float jy, float jz) {
+  const float rt = inside ? r - kTol : r + kTol;
+  const float b = 2 * (jx * dx + jy * dy + jz * dz);
+  const float c = dx * dx + dy * dy + dz * dz - rt * rt;
+  const float sq0 = b * b - 4 * a * c;
+  const bool miss = sq0 < 0;
+  const float sq = sqrtf(miss ? 0.0f : sq0);
+  float fpos, fneg;
+  roots(a, b, c, sq, fpos, fneg);
+  float f;
+  if (inside) {
+    f = ref_max(ref_max(fpos, fneg), 0);
+  } else if (fpos > 0 && fneg > 0) {
+    f = ref_min(fpos, fneg);
+  } else {
+    f = ((fpos < 0 && fneg < 0) || (b > 0)) ? kBig : 0.0f;
+  }
+  return miss ? (inside ? 0.0f : kBig) : f;
+}
+
 // The T2 weight exp(x) of sim3d_kernel.cu:473/485 for a float argument,
 // evaluated in double and rounded once to float: the correctly rounded value
 // in all but rare double-rounding cases, so it agrees with any correctly
@@ -282,6 +308,20 @@ __device__ __forceinline__ float step_out_t(float dx, float dy, float dz, float 
     if (sq < __uint_as_float(0x368637bdu) * a) return float(step_out_f64(dx, dy, dz, r, jx, jy, jz));  // 4e-6
   }
   return step_out(dx, dy, dz, r, a, jx, jy, jz);
+}
+
+template <bool T64>
+__device__ __forceinline__ float step_either_t(bool inside, float dx, float dy, float dz, float r, float a, float jx,
+                                               float jy, float jz) {
+  if (T64) {
+    const float rt = inside ? r - kTol : r + kTol;
+    const float b = 2 * (jx * dx + jy * dy + jz * dz);
+    const float c = dx * dx + dy * dy + dz * dz - rt * rt;
+    const float sq = b * b - 4 * a * c;
+    if (sq < __uint_as_float(0x368637bdu) * a)  // 4e-6
+      return float(inside ? step_in_f64(dx, dy, dz, r, jx, jy, jz) : step_out_f64(dx, dy, dz, r, jx, jy, jz));
+  }
+  return step_either(inside, dx, dy, dz, r, a, jx, jy, jz);
 }
 
 // Kahan-compensated accumulation.

@@ -94,13 +94,13 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
       const int k = start + base + i;
       const float4 c = __ldg(sph4 + k);
       const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
-      if (in_mask & (1u << i)) {
+      const bool inside = (in_mask >> i) & 1u;
+      const float f = step_either_t<T64>(inside, dx, dy, dz, c.w, a, jx, jy, jz);
+      if (inside) {
         o.any_in = true;
-        const float f = step_in_t<T64>(dx, dy, dz, c.w, a, jx, jy, jz);
         if (o.fin < f) o.fin = f;
-      } else {
-        const float f = step_out_t<T64>(dx, dy, dz, c.w, a, jx, jy, jz);
-        if (f < o.fout) o.fout = f;
+      } else if (f < o.fout) {
+        o.fout = f;
       }
     }
   }
@@ -120,6 +120,17 @@ __device__ __forceinline__ int label_of(const float4* __restrict__ sph4, const i
     }
   }
   return L;
+}
+
+// Cell of the walker at the start of a step and the cell's low corner.
+__device__ __forceinline__ int step_cell(const Grid& g, float x, float y, float z, float& lox, float& loy,
+                                         float& loz) {
+  float cx, cy, cz;
+  const int c = cell_of(g, x, y, z, cx, cy, cz);
+  lox = cx * g.dLx - g.Lx / 2;
+  loy = cy * g.dLy - g.Ly / 2;
+  loz = cz * g.dLz - g.Lz / 2;
+  return c;
 }
 
 // Draw `draw` of step s scaled by ds.
@@ -164,24 +175,19 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
   int s = s0;
   int niter = 0, draw = 0, cell = 0;
   float lox = 0.f, loy = 0.f, loz = 0.f;  // low corner of the step's cell
-  float jr = 1.0f, ds = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+  float jr = 1.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+  // ds depends on the label only; it is recomputed when the label at the
+  // start of a step differs from the one it was computed for
+  int ds_label = label;
+  float ds = sqrtf(2 * __ldg(J.D + label) * dt);
+  if (s < s1) {
+    cell = step_cell(J.g, x, y, z, lox, loy, loz);
+    jump_of(J, wid, s, 0, ds, jx, jy, jz);
+    draw = 1;
+  }
   while (s < s1) {
-    if (niter == 0) {
-      float cx, cy, cz;
-      cell = cell_of(J.g, x, y, z, cx, cy, cz);
-      lox = cx * J.g.dLx - J.g.Lx / 2;
-      loy = cy * J.g.dLy - J.g.Ly / 2;
-      loz = cz * J.g.dLz - J.g.Lz / 2;
-      jr = 1.0f;
-      draw = 0;
-    }
     niter++;
     float jc = jr;
-    if (niter == 1) {
-      ds = sqrtf(2 * __ldg(J.D + label) * dt);
-      jump_of(J, wid, s, 0, ds, jx, jy, jz);
-      draw = 1;
-    }
     float a = jx * jx + jy * jy + jz * jz;
     float reach = sqrtf(a) * jr;
     // Near list when everything this iteration can touch lies within its
@@ -205,6 +211,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
       label = label_of(sph4, sidv, start, count, J.nstructures, x, y, z);
       if (niter == 1) {  // the first draw's length depends on the label
         ds = sqrtf(2 * __ldg(J.D + label) * dt);
+        ds_label = label;
         jump_of(J, wid, s, 0, ds, jx, jy, jz);
         a = jx * jx + jy * jy + jz * jz;
         reach = sqrtf(a) * jr;
@@ -218,10 +225,13 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     x += jc * jx;
     y += jc * jy;
     z += jc * jz;
+    // the next draw: the scatter draw of this step, or the first draw of the
+    // next one; every iteration ends with one or the other, so one call site
+    // serves all lanes of the warp
+    int next_step = s, next_draw = draw;
     if (jc < jr) {
       jr = sqrtf(ref_max(0, jr * jr - jc * jc));
       if (MODE & NZ_MODE_SIG) sig *= t2_decay(-jc * jc * dt / __ldg(J.T2 + label));
-      jump_of(J, wid, s, draw, ds, jx, jy, jz);
       draw++;
     } else {
       jr -= jc;
@@ -282,7 +292,17 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
       }
       s++;
       niter = 0;
+      jr = 1.0f;
+      draw = 1;
+      next_step = s;
+      next_draw = 0;
+      if (label != ds_label) {
+        ds = sqrtf(2 * __ldg(J.D + label) * dt);
+        ds_label = label;
+      }
+      cell = step_cell(J.g, x, y, z, lox, loy, loz);
     }
+    if (s < s1) jump_of(J, wid, next_step, next_draw, ds, jx, jy, jz);
   }
   J.pos[w] = make_float4(x, y, z, __int_as_float(label));
   if (kMom) J.org[w] = make_float4(x0, y0, z0, __uint_as_float(wid));

@@ -34,6 +34,40 @@ def _dev():
     return torch.device("cuda", torch.cuda.current_device())
 
 
+def validate_substrate(sph64: np.ndarray, nstructures: int, L3, nseg, D, T2):
+    """Host-side checks of a substrate before any device work (the reference
+    checks none of these): finite centres, finite positive radii, structure
+    ids that are integers in [0, nstructures), a positive box, at least one
+    cell per axis, finite D >= 0 and T2 > 0 for every structure and the box.
+    Raises NozomiError naming the first problem."""
+    sph64 = np.asarray(sph64, dtype=np.float64)
+    if sph64.ndim != 2 or sph64.shape[0] != 5:
+        raise NozomiError(f"spheres must be [5, S] (cx, cy, cz, r, structure id), got {sph64.shape}")
+    if sph64.size:
+        bad = ~np.isfinite(sph64[:4]).all(axis=0)
+        if bad.any():
+            raise NozomiError(f"sphere {int(np.argmax(bad))} has a non-finite centre or radius")
+        if (sph64[3] <= 0).any():
+            raise NozomiError(f"sphere {int(np.argmax(sph64[3] <= 0))} has radius <= 0")
+        sid = sph64[4]
+        okid = np.isfinite(sid) & (sid == np.round(sid)) & (sid >= 0) & (sid < nstructures)
+        if not okid.all():
+            raise NozomiError(f"sphere {int(np.argmax(~okid))} has structure id {sid[np.argmax(~okid)]!r} "
+                              f"outside [0, {nstructures})")
+    Lv = np.asarray(L3, dtype=np.float64)
+    if Lv.shape != (3,) or not (np.isfinite(Lv).all() and (Lv > 0).all()):
+        raise NozomiError(f"box {tuple(L3)} must be three finite positive lengths")
+    if len(tuple(nseg)) != 3 or min(int(v) for v in nseg) < 1:
+        raise NozomiError(f"cell grid {tuple(nseg)} needs at least one cell per axis")
+    Dv, Tv = np.asarray(D, np.float64).ravel(), np.asarray(T2, np.float64).ravel()
+    if Dv.size != nstructures + 1 or Tv.size != nstructures + 1:
+        raise NozomiError("D and T2 need one entry per structure plus the box")
+    if not (np.isfinite(Dv).all() and (Dv >= 0).all()):
+        raise NozomiError("D must be finite and >= 0")
+    if not (np.isfinite(Tv).all() and (Tv > 0).all()):
+        raise NozomiError("T2 must be finite and > 0")
+
+
 def box_grid(L3, nseg) -> L.Grid:
     """The reference's float constants Lx.. and dLx = Lx / nseg (diffsim3d.py:115-120)."""
     Lx, Ly, Lz = (float(v) for v in L3)
@@ -49,9 +83,10 @@ class DeviceSubstrate:
 
     def __init__(self, spheres: np.ndarray, nstructures: int, L3, nseg, D, T2, jump_tol: float = 1.0,
                  cells: tuple | None = None, near_margin: float | None = None):
+        sph64 = np.ascontiguousarray(spheres, dtype=np.float64).reshape(5, -1)
+        validate_substrate(sph64, int(nstructures), L3, nseg, D, T2)
         require_cuda()
         dev = _dev()
-        sph64 = np.ascontiguousarray(spheres, dtype=np.float64).reshape(5, -1)
         self.S = sph64.shape[1]
         self.nstructures = int(nstructures)
         self.L = tuple(float(v) for v in L3)
@@ -63,8 +98,6 @@ class DeviceSubstrate:
         self.spheres = torch.from_numpy(sph64.astype(np.float32)).to(dev)
         self.D = torch.as_tensor(np.asarray(D, np.float32), device=dev)
         self.T2 = torch.as_tensor(np.asarray(T2, np.float32), device=dev)
-        if self.D.numel() != self.nstructures + 1 or self.T2.numel() != self.nstructures + 1:
-            raise NozomiError("D and T2 need one entry per structure plus the box")
         if cells is None:
             self._build_cells()
         else:

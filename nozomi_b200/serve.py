@@ -15,6 +15,13 @@ after their admission.
 
 Draws are keyed by (request seed, walker id, step), so a request's result is
 the one it gets alone (tests/test_serve.py).
+
+Failures stay with their request: a request whose substrate is invalid,
+whose target structures have no volume, or whose admission runs out of
+device memory completes at once with ``error`` set; ``cancel`` withdraws a
+waiting or resident request between rounds; a request with a deadline
+(seconds after arrival, a host-side watchdog checked every round) that is
+not done by then is cancelled with an error.  The other requests go on.
 """
 from __future__ import annotations
 
@@ -41,6 +48,7 @@ class Ticket:
     completed: float = None
     signal: np.ndarray = None
     error: str = None
+    deadline: float = None
     job: dict = field(default=None, repr=False)
 
     @property
@@ -79,11 +87,40 @@ class Server:
         self.clock = time.perf_counter
 
     # -- requests ------------------------------------------------------------------
-    def submit(self, spec: JobSpec, arrival: float | None = None) -> Ticket:
+    def submit(self, spec: JobSpec, arrival: float | None = None, deadline_s: float | None = None) -> Ticket:
+        """Queue a request; deadline_s: seconds after arrival after which it
+        is cancelled if not complete."""
         t = Ticket(self.next_id, spec, self.clock() if arrival is None else arrival)
+        if deadline_s is not None:
+            t.deadline = t.arrival + float(deadline_s)
         self.next_id += 1
         self.waiting.append(t)
         return t
+
+    def _fail(self, t: Ticket, why: str):
+        t.error = why
+        t.completed = self.clock()
+        if t.job is not None:
+            self.used -= t.job["bytes"]
+            t.job = None
+        self.done.append(t)
+
+    def cancel(self, t: Ticket, why: str = "cancelled") -> bool:
+        """Withdraw a waiting or resident request (between rounds: none of its
+        work is in flight then).  Returns False if it already completed."""
+        if t in self.waiting:
+            self.waiting.remove(t)
+        elif t in self.active:
+            self.active.remove(t)
+        else:
+            return False
+        self._fail(t, why)
+        return True
+
+    def _watchdog(self):
+        now = self.clock()
+        for t in [t for t in self.waiting + self.active if t.deadline is not None and now > t.deadline]:
+            self.cancel(t, f"deadline exceeded ({t.deadline - t.arrival:.3g} s after arrival)")
 
     def _admit(self):
         while self.waiting:
@@ -100,19 +137,20 @@ class Server:
                 dev = torch.device("cuda", torch.cuda.current_device())
                 targets = list(range(sub.nstructures + 1)) if sp.targets is None else list(sp.targets)
                 x, lab = engine.seed(sub, targets, sp.N, key=sp.seed ^ 0x5EED)
+                wk = engine.Walkers(x, x.clone(), phi=torch.zeros((6, sp.N), device=dev), label=lab)
+                j = {"sub": sub, "G": torch.from_numpy(G).to(dev), "Garea": torch.from_numpy(Ga).to(dev),
+                     "nsteps": int(G.size), "dt": float(sp.gwave.dt), "N": int(sp.N),
+                     "draws": engine.philox_draws(sp.seed, 0),
+                     "dirs": torch.as_tensor(np.asarray(sp.dirs, np.float32), device=dev).contiguous(),
+                     "amps": torch.as_tensor(np.asarray(sp.amplitudes, np.float32).ravel(), device=dev),
+                     "buf": [engine.FusedState.from_walkers(wk), engine.FusedState(sp.N)], "cur": 0,
+                     "scratch": None, "offset": 0, "bytes": need}
             except engine.NozomiError as e:  # a bad request fails alone; the others go on
-                t.error = str(e)
-                t.completed = self.clock()
-                self.done.append(t)
+                self._fail(t, str(e))
                 continue
-            wk = engine.Walkers(x, x.clone(), phi=torch.zeros((6, sp.N), device=dev), label=lab)
-            j = {"sub": sub, "G": torch.from_numpy(G).to(dev), "Garea": torch.from_numpy(Ga).to(dev),
-                 "nsteps": int(G.size), "dt": float(sp.gwave.dt), "N": int(sp.N),
-                 "draws": engine.philox_draws(sp.seed, 0),
-                 "dirs": torch.as_tensor(np.asarray(sp.dirs, np.float32), device=dev).contiguous(),
-                 "amps": torch.as_tensor(np.asarray(sp.amplitudes, np.float32).ravel(), device=dev),
-                 "buf": [engine.FusedState.from_walkers(wk), engine.FusedState(sp.N)], "cur": 0, "scratch": None,
-                 "offset": 0, "bytes": need}
+            except torch.cuda.OutOfMemoryError as e:  # so does one whose admission runs out of memory
+                self._fail(t, f"out of device memory at admission: {str(e).splitlines()[0]}")
+                continue
             t.job = j
             t.admitted = self.clock()
             self.used += need
@@ -122,6 +160,7 @@ class Server:
     def round(self):
         """Admit, advance every resident request by one chunk, retire the
         finished ones.  Returns the tickets completed in this round."""
+        self._watchdog()
         self._admit()
         if not self.active:
             return []
@@ -173,7 +212,7 @@ class Server:
             self.round()
         return self.done
 
-    def serve(self, requests, time_limit: float | None = None):
+    def serve(self, requests, time_limit: float | None = None, deadline_s: float | None = None):
         """Replay a request stream (workloads.Request list, arrival times in
         seconds from now) in real time; returns the completed tickets."""
         start = self.clock()
@@ -182,7 +221,7 @@ class Server:
         while i < len(pending) or self.waiting or self.active:
             now = self.clock() - start
             while i < len(pending) and pending[i].arrival <= now:
-                self.submit(pending[i].spec, start + pending[i].arrival)
+                self.submit(pending[i].spec, start + pending[i].arrival, deadline_s=deadline_s)
                 i += 1
             if not self.waiting and not self.active:
                 time.sleep(max(0.0, min(0.01, pending[i].arrival - now)) if i < len(pending) else 0)

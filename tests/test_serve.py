@@ -73,3 +73,50 @@ def test_bad_request_fails_alone():
     tg = srv.submit(_spec(0, 10, 1000, 200, 6))
     srv.drain()
     assert tb.error is not None and tg.error is None and tg.signal is not None
+
+
+def test_cancel_deadline_oom_and_invalid_substrate_fail_alone(monkeypatch):
+    """Host-side failure injection: a request cancelled while resident, one
+    past its deadline, one whose admission runs out of device memory (a fake
+    allocation failure) and one with a NaN radius each end with an error; the
+    others complete with the result they get alone."""
+    from nozomi_b200 import engine
+    from nozomi_b200.batch import BatchRun, JobSpec, SubstrateCache
+    from nozomi_b200.serve import Server
+    from nozomi_b200.simulate import Tuning
+    from nozomi_b200.substrates import axon_bundle
+    tuning = Tuning(steps_per_launch=100)
+    good = [_spec(i, 10, 1500, 400, 6) for i in range(3)]
+    victim = _spec(7, 10, 2000, 600, 6)  # same cache key and substrate as good[1]
+    late = _spec(8, 10, 1000, 300, 6)
+    oom = _spec(9, 10, 1000, 300, 6)
+    nan_sub = axon_bundle(10, seed=3)
+    f0 = np.array(nan_sub.fibers[0], dtype=np.float64)
+    f0[0, 3] = np.nan
+    nan_sub.fibers[0] = f0
+    nan_req = JobSpec(nan_sub, good[0].gwave, good[0].dirs, good[0].amplitudes, 1000, seed=5, key="nan")
+    real_seed = engine.seed
+
+    def seed(sub, targets, N, key, **kw):
+        if key == oom.seed ^ 0x5EED:
+            raise torch.cuda.OutOfMemoryError("injected: CUDA out of memory")
+        return real_seed(sub, targets, N, key, **kw)
+    monkeypatch.setattr(engine, "seed", seed)
+    srv = Server(tuning=tuning, threads=128)
+    tg = [srv.submit(good[0]), srv.submit(victim)]
+    srv.round()
+    assert srv.cancel(tg[1]) and not srv.cancel(tg[1])
+    tl = srv.submit(late, deadline_s=0.0)
+    to, tn = srv.submit(oom), srv.submit(nan_req)
+    tg += [srv.submit(good[1]), srv.submit(good[2])]
+    srv.drain()
+    assert tg[1].error == "cancelled"
+    assert tl.error.startswith("deadline exceeded")
+    assert to.error.startswith("out of device memory at admission")
+    assert "non-finite" in tn.error
+    assert srv.used == 0 and not srv.active and not srv.waiting
+    cache = SubstrateCache()
+    for t, sp in zip([tg[0], tg[2], tg[3]], good):
+        assert t.error is None
+        alone = BatchRun([sp], tuning=tuning, threads=64, cache=cache).step().signals()[0]
+        np.testing.assert_allclose(t.signal, alone, rtol=0, atol=1e-12)
