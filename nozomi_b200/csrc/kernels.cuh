@@ -44,7 +44,7 @@ constexpr int kFusedMaxThreads = 256;  // largest CTA of nz_walk_batch
 #define NZ_FUSED_MIN_BLOCKS 3
 #endif
 #ifndef NZ_SCAN_BATCH
-#define NZ_SCAN_BATCH 4
+#define NZ_SCAN_BATCH 1
 #endif
 constexpr int kFusedMinBlocks = NZ_FUSED_MIN_BLOCKS;  // 256-thread CTAs per SM the register budget is sized for
 constexpr int kScanBatch = NZ_SCAN_BATCH;             // cell-list entries loaded together per thread

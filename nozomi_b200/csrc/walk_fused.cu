@@ -41,7 +41,7 @@ struct ScanOut {
 // walker's label is not L (then nothing in `o` is used).  The entries of a
 // cell are ordered by structure id: the pass ends at the first entry of a
 // structure above L (the reference skips those spheres, :805-806).  Entries
-// are read kScanBatch at a time so that several loads are in flight per thread.
+// are read kScanBatch at a time (1 measured fastest on the packed workload).
 template <bool T64>
 __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const int* __restrict__ sid, int start,
                                           int count, int nstructures, float x, float y, float z, int L, float a,
@@ -50,6 +50,9 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
   o.fout = kBig;
   o.any_in = false;
   bool found = false, lower = false, stop = false;
+  // A walker in the box (label nstructures) has every entry below its label:
+  // nothing to stop at and no structure id to read.
+  const bool box = L >= nstructures;
   const float slack = kTol + reach * 1.02f + 2e-3f;
   for (int base = 0; base < count && !stop; base += 32) {
     const int m = min(32, count - base);
@@ -61,30 +64,33 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
       for (int u = 0; u < kScanBatch; ++u) {
         const int k = start + base + i0 + u;
         if (i0 + u < m) {
-          sv[u] = __ldg(sid + k);
+          sv[u] = box ? -1 : __ldg(sid + k);
           cv[u] = __ldg(sph4 + k);
         } else {
           sv[u] = 0x7fffffff;
+          cv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
       }
+      // Predicated, without branches: an entry is near when within
+      // (r + slack), a slack of at least 2.1 nm that dwarfs the rounding of
+      // d2 and r*r, so a far sphere neither contains the walker nor lies
+      // within this iteration's reach; only near entries take the
+      // reference's inside test.
 #pragma unroll
       for (int u = 0; u < kScanBatch; ++u) {
         const int s = sv[u];
-        if (s > L) {
-          stop = true;
-        } else {
-          const float dx = x - cv[u].x, dy = y - cv[u].y, dz = z - cv[u].z;
-          const float d2 = dx * dx + dy * dy + dz * dz;
-          const uint32_t bit = 1u << (i0 + u);
-          if (d2 - cv[u].w * cv[u].w < 0) {
-            in_mask |= bit;
-            if (s < L) lower = true;
-            else found = true;
-          } else if (s < L) {
-            const float t = cv[u].w + slack;
-            if (d2 <= t * t) out_mask |= bit;
-          }
-        }
+        const bool valid = s <= L;
+        stop |= !valid;
+        const float dx = x - cv[u].x, dy = y - cv[u].y, dz = z - cv[u].z;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        const float t = cv[u].w + slack;
+        const bool nb = valid && (d2 <= t * t);
+        const bool ins = nb && (d2 - cv[u].w * cv[u].w < 0);
+        const uint32_t bit = 1u << (i0 + u);
+        in_mask |= ins ? bit : 0u;
+        out_mask |= (nb && !ins && s < L) ? bit : 0u;
+        lower |= ins && (s < L);
+        found |= ins && (s >= L);
       }
     }
     uint32_t todo = in_mask | out_mask;
