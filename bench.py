@@ -42,6 +42,12 @@ WORKLOAD = ("packed substrate: 200 beaded axons x 100 spheres (lognormal r0 1.0/
             "PGSE delta=10 Delta=20 te=30 ms at dt=5 us (6000 steps), 30 directions x b={0,1,2,3} ms/um^2")
 
 
+# the configuration profiled with ncu and its DRAM read + write bytes per
+# walk_fused_kernel launch (1e6 walkers x 1000 steps)
+PROFILED_SHAPE = (1_000_000, 0.5, 0.5, 1000)
+PROFILED_TRAFFIC_BYTES = 4_385_864_000 + 70_056_960
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -301,7 +307,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     engine.require_cuda()
     sub, pg, dirs, bvals = workload()
-    tuning = Tuning()
+    # launch shape tuned for this workload (profiles/walk_fused_packed_tuning.md):
+    # 0.5 um cells, near margin 0.5 um, re-binning bins of 8^3 cells, 1000 steps per launch
+    tuning = Tuning(cell=0.5, near_margin=0.5, coarsen=8, steps_per_launch=1000)
     if args.cell:
         tuning.cell = args.cell
     if args.steps_per_launch:
@@ -452,8 +460,13 @@ def run_ours(args):
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         # HBM view: walker state read + written once per launch (4 x float4 each way)
         state_bytes = N * 128
+        # DRAM bytes of one launch from an ncu capture of this configuration
+        # (profiles/walk_fused_packed1e6_ncu.md); none for other shapes
+        traffic = None
+        if (N, tuning.cell, tuning.near_margin, tuning.steps_per_launch) == PROFILED_SHAPE:
+            traffic = PROFILED_TRAFFIC_BYTES
         roof_hbm = {"bound": "hbm", "achieved": state_bytes / (walk_launch_ms * 1e-3) / 1e9, "peak": hbm_peak,
-                    "unit": "GB/s", "traffic": None,
+                    "unit": "GB/s", "traffic": traffic, "algorithmic_bytes_per_launch": state_bytes,
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk.exists() else "fallback 6.65 TB/s"}
         roof_hbm["frac"] = roof_hbm["achieved"] / hbm_peak
         roof_fp32 = None
