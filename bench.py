@@ -559,12 +559,15 @@ def run_batched(args):
     ws = run.walker_steps()
     value = ws * args.steps / (ms * 1e-3)
     sig_batched = run.signals()
-    # the plain per-substrate path, one job after another, launched from the host
+    # the plain per-substrate path, one job after another, launched from the
+    # host, on cell lists of the default shape (1 um cells; not the batch's
+    # tuned shape, which the plain kernel does not benefit from)
     sel = list(range(0, len(specs), args.plain_every))
     plain_ms, plain_ws, err = 0.0, 0, 0.0
+    plain_tuning, plain_cache = Tuning(), SubstrateCache()
     for i in sel:
         sp = specs[i]
-        dsub = cache.get(sp.key, sp.substrate, sp.D, sp.T2, tuning)
+        dsub = plain_cache.get(sp.key, sp.substrate, sp.D, sp.T2, plain_tuning)
         x = run.positions[i][0]
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -591,7 +594,8 @@ def run_batched(args):
                 "trial_walker_steps_per_s": tune_report.get("trial_walker_steps_per_s")},
             "gpu_launches": run.launches() * args.steps,
             "plain": {"value": plain_value, "unit": "walker-steps/s", "jobs_timed": len(sel),
-                      "walker_steps_timed": plain_ws, "launch": "one plain-kernel launch per step from the host, "
+                      "walker_steps_timed": plain_ws, "cell_um": plain_tuning.cell,
+                      "launch": "one plain-kernel launch per step from the host, "
                       "per-direction phase in HBM, substrates one after another"},
             "speedup_vs_plain": value / plain_value,
             "max_signal_diff_batched_vs_plain": err, "clocks": clk}

@@ -25,10 +25,10 @@ from .waveforms import ArbitraryWaveform
 
 SPACE = {
     "threads": [64, 128, 256],
-    "cell": [1.0, 1.5],
+    "cell": [0.5, 0.667, 1.0, 1.5],
     "near_margin": [0.4, 0.5, 0.6, None],
     "steps_per_launch": [250, 500, 1000, 2000],
-    "coarsen": [2, 4, 8],
+    "coarsen": [2, 4, 8, 12],
 }
 CACHE_FILE = Path(os.environ.get("NOZOMI_B200_CACHE", Path.home() / ".cache" / "nozomi_b200")) / "autotune.json"
 
@@ -97,7 +97,8 @@ def autotune(specs, space=None, trial_steps: int = 2000, max_walkers: int = 50_0
         return v
 
     best = measure(cur)
-    for name in ["near_margin", "threads", "steps_per_launch", "coarsen", "cell"]:
+    # the cell edge first (the best re-binning coarsening and near margin depend on it)
+    for name in ["cell", "coarsen", "near_margin", "threads", "steps_per_launch"]:
         for val in space[name]:
             if val == cur[name]:
                 continue
