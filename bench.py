@@ -46,6 +46,7 @@ WORKLOAD = ("packed substrate: 200 beaded axons x 100 spheres (lognormal r0 1.0/
 # walk_fused_kernel launch (1e6 walkers x 1000 steps)
 PROFILED_SHAPE = (1_000_000, 0.5, 0.5, 1000)
 PROFILED_TRAFFIC_BYTES = 4_385_864_000 + 70_056_960
+PROFILED_WARP_INST_PER_WALKER_STEP = 64.9
 
 
 def parse():
@@ -308,8 +309,8 @@ def run_ours(args):
     engine.require_cuda()
     sub, pg, dirs, bvals = workload()
     # launch shape tuned for this workload (profiles/walk_fused_packed_tuning.md):
-    # 0.5 um cells, near margin 0.5 um, re-binning bins of 8^3 cells, 1000 steps per launch
-    tuning = Tuning(cell=0.5, near_margin=0.5, coarsen=8, steps_per_launch=1000)
+    # 0.5 um cells, near margin 0.5 um, re-binning bins of 8^3 cells, 2000 steps per launch
+    tuning = Tuning(cell=0.5, near_margin=0.5, coarsen=8, steps_per_launch=2000)
     if args.cell:
         tuning.cell = args.cell
     if args.steps_per_launch:
@@ -476,6 +477,16 @@ def run_ours(args):
             roof_fp32 = {"bound": "fp32", "achieved": ach, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
                          "frac": ach / fp32_peak_tflops, "flops_per_walker_step": F_alg, "work_per_walker_step": wk,
                          "peak_source": "nz_probe_fma on this GPU (8 FFMA chains/thread)"}
+        # the bound that binds this kernel: instruction issue (4 warp-instructions
+        # per SM per cycle), with the warp-instructions per walker-step counted
+        # by ncu for the profiled shape
+        roof_issue = None
+        if traffic is not None and clk and clk.get("sm_mhz"):
+            peak = sms * 4 * clk["sm_mhz"] * 1e6
+            ach = PROFILED_WARP_INST_PER_WALKER_STEP * kernel_ws_s
+            roof_issue = {"bound": "issue", "achieved": ach, "peak": peak, "unit": "warp-instructions/s",
+                          "frac": ach / peak, "warp_instructions_per_walker_step": PROFILED_WARP_INST_PER_WALKER_STEP,
+                          "peak_source": f"{sms} SMs x 4 issue slots x median SM clock under load"}
         line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -498,7 +509,8 @@ def run_ours(args):
                            "share_of_step": walk_ms / eager_ms, "eager_step_ms": eager_ms,
                            "timing": "value from CUDA-graph replays of the step; kernel figures from one eager "
                                      "step with events around each fused launch"},
-                "roofline": roof_hbm, "roofline_fp32": roof_fp32, "cpu_baseline": cpu, "clocks": clk,
+                "roofline": roof_hbm, "roofline_fp32": roof_fp32, "roofline_issue": roof_issue,
+                "cpu_baseline": cpu, "clocks": clk,
                 "signal_b0_mean": float(np.mean(np.abs(S[:, 0]))),
                 "signal_mean_by_b": [float(np.mean(S[:, b].real)) for b in range(S.shape[1])]}
         print(json.dumps(line), flush=True)

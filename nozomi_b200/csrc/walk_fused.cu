@@ -56,7 +56,11 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
   const float slack = kTol + reach * 1.02f + 2e-3f;
   for (int base = 0; base < count && !stop; base += 32) {
     const int m = min(32, count - base);
-    uint32_t in_mask = 0u, out_mask = 0u;
+    // first pass: which entries are near, i.e. within (r + slack), a slack of
+    // at least 2.1 nm that dwarfs the rounding of d2 and r*r, so that a far
+    // sphere neither contains the walker nor lies within this iteration's
+    // reach; predicated, one entry per load
+    uint32_t near_mask = 0u;
     for (int i0 = 0; i0 < m && !stop; i0 += kScanBatch) {
       int sv[kScanBatch];
       float4 cv[kScanBatch];
@@ -71,42 +75,37 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
           cv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
       }
-      // Predicated, without branches: an entry is near when within
-      // (r + slack), a slack of at least 2.1 nm that dwarfs the rounding of
-      // d2 and r*r, so a far sphere neither contains the walker nor lies
-      // within this iteration's reach; only near entries take the
-      // reference's inside test.
 #pragma unroll
       for (int u = 0; u < kScanBatch; ++u) {
-        const int s = sv[u];
-        const bool valid = s <= L;
+        const bool valid = sv[u] <= L;
         stop |= !valid;
         const float dx = x - cv[u].x, dy = y - cv[u].y, dz = z - cv[u].z;
         const float d2 = dx * dx + dy * dy + dz * dz;
         const float t = cv[u].w + slack;
-        const bool nb = valid && (d2 <= t * t);
-        const bool ins = nb && (d2 - cv[u].w * cv[u].w < 0);
-        const uint32_t bit = 1u << (i0 + u);
-        in_mask |= ins ? bit : 0u;
-        out_mask |= (nb && !ins && s < L) ? bit : 0u;
-        lower |= ins && (s < L);
-        found |= ins && (s >= L);
+        near_mask |= (valid && d2 <= t * t) ? (1u << (i0 + u)) : 0u;
       }
     }
-    uint32_t todo = in_mask | out_mask;
-    while (todo) {
-      const int i = __ffs(todo) - 1;
-      todo &= todo - 1;
+    // second pass, near entries only: the reference's inside test, then the
+    // fraction of a containing sphere or of a lower structure's sphere
+    while (near_mask) {
+      const int i = __ffs(near_mask) - 1;
+      near_mask &= near_mask - 1;
       const int k = start + base + i;
       const float4 c = __ldg(sph4 + k);
+      const int s = box ? -1 : __ldg(sid + k);
       const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
-      const bool inside = (in_mask >> i) & 1u;
-      const float f = step_either_t<T64>(inside, dx, dy, dz, c.w, a, jx, jy, jz);
-      if (inside) {
-        o.any_in = true;
-        if (o.fin < f) o.fin = f;
-      } else if (f < o.fout) {
-        o.fout = f;
+      const float d2 = dx * dx + dy * dy + dz * dz;
+      const bool inside = d2 - c.w * c.w < 0;
+      lower |= inside && (s < L);
+      found |= inside && (s >= L);
+      if (inside || s < L) {
+        const float f = step_either_t<T64>(inside, dx, dy, dz, c.w, a, jx, jy, jz);
+        if (inside) {
+          o.any_in = true;
+          if (o.fin < f) o.fin = f;
+        } else if (f < o.fout) {
+          o.fout = f;
+        }
       }
     }
   }
