@@ -80,7 +80,9 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
         const bool valid = sv[u] <= L;
         stop |= !valid;
         const float dx = x - cv[u].x, dy = y - cv[u].y, dz = z - cv[u].z;
-        const float d2 = dx * dx + dy * dy + dz * dz;
+        // a filter, not the reference's arithmetic: fused multiply-adds are
+        // fine here (their rounding is far inside the slack)
+        const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
         const float t = cv[u].w + slack;
         near_mask |= (valid && d2 <= t * t) ? (1u << (i0 + u)) : 0u;
       }
