@@ -42,11 +42,12 @@ WORKLOAD = ("packed substrate: 200 beaded axons x 100 spheres (lognormal r0 1.0/
             "PGSE delta=10 Delta=20 te=30 ms at dt=5 us (6000 steps), 30 directions x b={0,1,2,3} ms/um^2")
 
 
-# the configuration profiled with ncu and its DRAM read + write bytes per
-# walk_fused_kernel launch (1e6 walkers x 1000 steps)
-PROFILED_SHAPE = (1_000_000, 0.5, 0.5, 1000)
-PROFILED_TRAFFIC_BYTES = 4_385_864_000 + 70_056_960
-PROFILED_WARP_INST_PER_WALKER_STEP = 64.9
+# the configuration profiled with ncu, its DRAM read + write bytes per
+# walk_fused_kernel launch (1e6 walkers x 2000 steps) and its warp
+# instructions per walker-step
+PROFILED_SHAPE = (1_000_000, 0.5, 0.5, 2000)
+PROFILED_TRAFFIC_BYTES = 9_966_812_000 + 94_345_472
+PROFILED_WARP_INST_PER_WALKER_STEP = 56.5
 
 
 def parse():
