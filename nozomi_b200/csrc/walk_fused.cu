@@ -181,6 +181,10 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
   const bool has_near = J.near_sph4 != nullptr;
   int s = s0;
   int niter = 0, draw = 0, cell = 0;
+  // start and count of the step cell's primary list (the near list where
+  // there is one), loaded as soon as the cell is known so that the load
+  // overlaps the draw
+  int pstart = 0, pcount = 0;
   float lox = 0.f, loy = 0.f, loz = 0.f;  // low corner of the step's cell
   float jr = 1.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
   // ds depends on the label only; it is recomputed when the label at the
@@ -189,6 +193,8 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
   float ds = sqrtf(2 * __ldg(J.D + label) * dt);
   if (s < s1) {
     cell = step_cell(J.g, x, y, z, lox, loy, loz);
+    pstart = __ldg((has_near ? J.near_start : J.cell_start) + cell);
+    pcount = __ldg((has_near ? J.near_count : J.cell_count) + cell);
     jump_of(J, wid, s, 0, ds, jx, jy, jz);
     draw = 1;
   }
@@ -210,8 +216,11 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     }
     const float4* sph4 = near ? J.near_sph4 : J.sph4;
     const int* sidv = near ? J.near_sid : J.sid;
-    const int start = __ldg((near ? J.near_start : J.cell_start) + cell);
-    const int count = __ldg((near ? J.near_count : J.cell_count) + cell);
+    int start = pstart, count = pcount;
+    if (has_near && !near) {
+      start = __ldg(J.cell_start + cell);
+      count = __ldg(J.cell_count + cell);
+    }
     ScanOut r;
     constexpr bool kT64 = (MODE & NZ_MODE_TANGENT64) != 0;
     if (!scan_cell<kT64>(sph4, sidv, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r)) {
@@ -308,6 +317,8 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
         ds_label = label;
       }
       cell = step_cell(J.g, x, y, z, lox, loy, loz);
+      pstart = __ldg((has_near ? J.near_start : J.cell_start) + cell);
+      pcount = __ldg((has_near ? J.near_count : J.cell_count) + cell);
     }
     if (s < s1) jump_of(J, wid, next_step, next_draw, ds, jx, jy, jz);
   }
