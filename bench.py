@@ -69,9 +69,12 @@ def parse():
     ap.add_argument("--coarsen", type=int, default=None)
     ap.add_argument("--by-label", type=int, default=None, help="re-bin by (label, bin): 1, or by bin only: 0")
     ap.add_argument("--near-margin", type=float, default=None, help="near-list margin in um (0: none)")
-    ap.add_argument("--workload", default="packed", choices=["packed", "batched", "serving"],
+    ap.add_argument("--narrow-walkers", type=float, default=5e5, help="narrow: walkers")
+    ap.add_argument("--narrow-ms", type=float, default=100.0, help="narrow: simulated time, ms")
+    ap.add_argument("--workload", default="packed", choices=["packed", "batched", "serving", "narrow"],
                     help="packed: one packed substrate (default); batched: 64 mixed substrates, batched vs plain; "
-                         "serving: Poisson request streams, continuous batching, p50/p99 latency")
+                         "serving: Poisson request streams, continuous batching, p50/p99 latency; "
+                         "narrow: the narrow-pulse simulation CLI path on a calibration-like substrate")
     ap.add_argument("--rates", default="5,20,50,100,200", help="serving: request rates (req/s)")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="serving: arrival window per rate")
     ap.add_argument("--max-requests", type=int, default=200, help="serving: requests per rate at most")
@@ -746,6 +749,80 @@ def run_reference_gpu(args):
     return 0
 
 
+NARROW_WORKLOAD = ("narrow-pulse D(t)/K(t) simulation through the drop-in API (the simulation CLI path): "
+                   "500 beaded axons (base diameter 1.68/0.45 um, beads +20-50 %, spheres every 0.5 um) packed "
+                   "to VF 0.65 in a periodic 50 um cube, 5e5 intra-axonal walkers, D=2.25 um^2/ms, dt=2 us, "
+                   "100 ms (5e4 steps), T2 weighting and displacement moments every step, nseg 20")
+# The reference's published run of this kind: 5e5 spins x 5e4 steps in about
+# 1 h at nseg 20 (docs/2_calibration.md:103; RTX A5000, wall time including
+# table build and I/O): 6.94e6 walker-steps/s.
+NARROW_PUBLISHED = 5e5 * 5e4 / 3600.0
+
+
+def run_narrow(args):
+    """The simulation CLI's work (cli/simulation_main.py): DiffSim3d with
+    set_segments(20, 20, 20), intra-axonal seeding, then every step walked
+    with its displacement moments on the device.  `value` from CUDA events
+    around the walk; `e2e` from the wall clock of set-up plus walk plus the
+    moments copied back, like the reference's TABLEtime + SIMtime."""
+    import torch
+    from nozomi_b200 import engine
+    from nozomi_b200.cli.simulation_main import narrow_pulse
+    from nozomi_b200.diffsim3d import DiffSim3d
+    from nozomi_b200.workloads import calibration_substrate
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    engine.require_cuda()
+    sub = calibration_substrate()
+    N, dt, sim_time = int(args.narrow_walkers), 0.002, float(args.narrow_ms)
+    nt = int(round(sim_time / dt))
+    geom = sub.geometry(D=2.25, T2=100.0)
+    stream = torch.cuda.current_stream()
+    runs = []
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            clocks.start()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        sim = DiffSim3d(geom, N)
+        sim.set_segments(20, 20, 20)
+        sim.setup(structures=list(range(sub.nstructures)), initstates_int=1234 + i)
+        torch.cuda.synchronize()
+        w1 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t, Dv, K = narrow_pulse(sim, nt, dt)  # ends with the moments copied to the host
+        e1.record(stream)
+        torch.cuda.synchronize()
+        w2 = time.perf_counter()
+        if i >= args.warmup:
+            runs.append({"table_s": w1 - w0, "walk_ms": e0.elapsed_time(e1), "wall_s": w2 - w0,
+                         "D_end": Dv[-1].tolist(), "K_end": K[-1].tolist()})
+        del sim
+    clk = clocks.stop()
+    ws = N * nt
+    walk_ms = float(np.mean([r["walk_ms"] for r in runs]))
+    wall_s = float(np.mean([r["wall_s"] for r in runs]))
+    value = ws / (walk_ms * 1e-3)
+    e2e = ws / wall_s
+    line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": walk_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": e2e / NARROW_PUBLISHED, "dtype": "f32",
+            "data": "synthetic (seeded packed substrate, seeded walkers)",
+            "config": {"workload": NARROW_WORKLOAD, "walkers": N, "time_steps": nt, "spheres": sub.S,
+                       "volume_fraction": sub.meta.get("volume_fraction"),
+                       "vs_baseline_basis": "e2e / 6.94e6 walker-steps/s, the reference's published run of "
+                                            "this kind (RTX A5000, wall time incl. set-up)"},
+            "e2e": {"value": e2e, "unit": "walker-steps/s",
+                    "h2d_bytes_per_step": int(sub.S * 5 * 8), "d2h_bytes_per_step": int(nt * 6 * 8),
+                    "wall_s": wall_s, "table_s": float(np.mean([r["table_s"] for r in runs]))},
+            "runs": runs, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -756,6 +833,8 @@ def main():
         return run_batched(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "narrow":
+        return run_narrow(args)
     return run_ours(args)
 
 

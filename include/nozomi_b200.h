@@ -215,6 +215,20 @@ int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mode, float d
                   const float* Garea, int step0, int step1, const nz_draws* draws, double* moments,
                   void* stream);
 
+/* ---- a8: the narrow-pulse loop — randomWalk3d then
+ * computeDiffusionCoefficientsAndKurtosis every step (simulation_main.py:91-118,
+ * sim3d_kernel.cu:162-238) — as one fused launch plus one reduction.  The walk
+ * (mode 0 or NZ_MODE_SIG) stores each walker's float displacement from its
+ * origin at the end of every step into scratch ([step1-step0][3][N] floats,
+ * nz_walk_fused_moments_scratch_bytes); a reduction kernel then adds, for each
+ * step s, the FP64 sums of dx^2, dy^2, dz^2, dx^4, dy^4, dz^4 over walkers to
+ * moments[s*6 .. s*6+5] (zeroed by the caller), the terms of nz_moments.  Any
+ * number of steps per call (at most 65535); the scratch grows with them. */
+size_t nz_walk_fused_moments_scratch_bytes(int N, int nsteps);
+int nz_walk_fused_moments(const nz_substrate* sub, const nz_state* st, int mode, float dt, const float* G,
+                          const float* Garea, int step0, int step1, const nz_draws* draws, float* scratch,
+                          size_t scratch_bytes, double* moments, void* stream);
+
 /* ---- batched persistent walk: every item of every job, steps [step0, step1)
  * of each job (clamped to its nsteps), CTAs pulling items from *queue (one
  * device int, zeroed by the caller) until none is left.  jobs and items are

@@ -75,6 +75,8 @@ SIGNATURES = {
     "nz_state_unpack": (_i, [_P, _P, _P]),
     "nz_state_unpack_by_id": (_i, [_P, _P, _P, _P]),
     "nz_walk_fused": (_i, [_P, _P, _i, _f, _P, _P, _i, _i, _P, _P, _P]),
+    "nz_walk_fused_moments_scratch_bytes": (ctypes.c_size_t, [_i, _i]),
+    "nz_walk_fused_moments": (_i, [_P, _P, _i, _f, _P, _P, _i, _i, _P, _P, ctypes.c_size_t, _P, _P]),
     "nz_walk_batch": (_i, [_P, _i, _P, _i, _i, _i, _i, _P, _i, _i, _P]),
     "nz_batch_occupancy": (_i, [_i, _i, _P]),
     "nz_sort_scratch_bytes": (ctypes.c_size_t, [_i, _i]),

@@ -180,6 +180,39 @@ extern "C" int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mo
                       static_cast<cudaStream_t>(stream));
 }
 
+extern "C" size_t nz_walk_fused_moments_scratch_bytes(int N, int nsteps) {
+  return (N > 0 && nsteps > 0) ? size_t(N) * 3 * size_t(nsteps) * sizeof(float) : 0;
+}
+
+extern "C" int nz_walk_fused_moments(const nz_substrate* sub, const nz_state* st, int mode, float dt, const float* G,
+                                     const float* Garea, int step0, int step1, const nz_draws* draws, float* scratch,
+                                     size_t scratch_bytes, double* moments, void* stream) {
+  int rc = check_fused_sub(sub, "nz_walk_fused_moments");
+  if (rc) return rc;
+  rc = check_state(st, "nz_walk_fused_moments");
+  if (rc) return rc;
+  if (!draws || draws->table)
+    return set_error(NZ_ERR_ARG, "nz_walk_fused_moments: Philox draws only (table must be NULL)");
+  if (mode & ~NZ_MODE_SIG) return set_error(NZ_ERR_ARG, "nz_walk_fused_moments: mode is 0 or NZ_MODE_SIG");
+  if ((mode & NZ_MODE_SIG) && !sub->T2) return set_error(NZ_ERR_ARG, "nz_walk_fused_moments: sig mode needs T2");
+  if (step0 < 0 || step1 < step0 || !moments) return set_error(NZ_ERR_ARG, "nz_walk_fused_moments: bad arguments");
+  if (st->N == 0 || step1 == step0) return NZ_OK;
+  const size_t need = nz_walk_fused_moments_scratch_bytes(st->N, step1 - step0);
+  if (!scratch || scratch_bytes < need || (reinterpret_cast<uintptr_t>(scratch) & 3))
+    return set_error(NZ_ERR_ARG, "nz_walk_fused_moments: scratch needs %zu bytes (4-byte aligned), got %zu", need,
+                     scratch_bytes);
+  if (step1 - step0 > 65535) return set_error(NZ_ERR_ARG, "nz_walk_fused_moments: at most 65535 steps per call");
+  const cudaStream_t cs = static_cast<cudaStream_t>(stream);
+  JobDev j = make_job(*sub, G, Garea, step1, dt, *draws, mode, *st, nullptr);
+  j.disp = scratch;
+  const int n_items = (st->N + kFusedThreads - 1) / kFusedThreads;
+  rc = launch_fused(mode | kModeDisp, j, nullptr, nullptr, n_items, step0, step1, nullptr, n_items, kFusedThreads, cs);
+  if (rc) return rc;
+  const int gx = min(64, (st->N + 255) / 256);
+  disp_moments_kernel<<<dim3(gx, step1 - step0), 256, 0, cs>>>(scratch, st->N, moments + size_t(step0) * 6);
+  return check_launch("disp_moments_kernel");
+}
+
 extern "C" int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0,
                              int step1, int* queue, int grid, int threads, void* stream) {
   if (!jobs || n_jobs <= 0 || !items || n_items < 0 || step0 < 0 || step1 < step0 || grid < 0)

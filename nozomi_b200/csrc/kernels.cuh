@@ -49,6 +49,10 @@ constexpr int kFusedMaxThreads = 256;  // largest CTA of nz_walk_batch
 constexpr int kFusedMinBlocks = NZ_FUSED_MIN_BLOCKS;  // 256-thread CTAs per SM the register budget is sized for
 constexpr int kScanBatch = NZ_SCAN_BATCH;             // cell-list entries loaded together per thread
 constexpr int kMomentSteps = 256;  // steps per launch in NZ_MODE_MOMENTS (shared-memory staging)
+// Internal mode bit (nz_walk_fused_moments only): at each step end the fused
+// walk stores the walker's float displacement from its origin; a reduction
+// kernel then forms the moments.
+constexpr int kModeDisp = 32;
 
 struct JobDev {
   Grid g;
@@ -70,6 +74,7 @@ struct JobDev {
   float4* phi;
   float4* comp;
   double* moments;
+  float* disp;  // kModeDisp: per-step displacements [steps of the launch][3][nwalkers]
   int nwalkers;
   int step_offset;
   // near lists (null sph4: none)
@@ -86,6 +91,7 @@ int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_it
                  int step1, int* queue, int grid, int threads, cudaStream_t st);
 int occupancy_fused(int mode, int threads, int* blocks_per_sm);
 __global__ void pack_kernel(nz_walkers wk, const uint32_t* ids, nz_state st);
+__global__ void disp_moments_kernel(const float* __restrict__ disp, int N, double* __restrict__ out);
 __global__ void unpack_kernel(nz_state st, nz_walkers wk, int by_id, int* bad);
 
 // ---- cells.cu ----

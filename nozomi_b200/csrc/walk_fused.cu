@@ -157,6 +157,8 @@ __device__ __forceinline__ void jump_of(const JobDev& J, uint32_t wid, int s, in
 template <int MODE>
 __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1, float* s_mom) {
   constexpr bool kMom = (MODE & NZ_MODE_MOMENTS) != 0;
+  constexpr bool kDisp = (MODE & kModeDisp) != 0;
+  constexpr bool kOrig = kMom || kDisp;  // origin in registers
   const float4 P = J.pos[w];
   float x = P.x, y = P.y, z = P.z;
   int label = __float_as_int(P.w);
@@ -171,7 +173,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     kx = C.x; ky = C.y; kz = C.z;
   }
   float x0 = 0.f, y0 = 0.f, z0 = 0.f;
-  if (kMom) {
+  if (kOrig) {
     const float4 O = J.org[w];
     x0 = O.x; y0 = O.y; z0 = O.z;
   }
@@ -267,7 +269,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
       const float Lx = J.g.Lx, Ly = J.g.Ly, Lz = J.g.Lz;
       if (fabsf(x) > Lx / 2 || fabsf(y) > Ly / 2 || fabsf(z) > Lz / 2) {  // rare: a wrap
         const float Ga = (MODE & NZ_MODE_PHI) ? __ldg(J.Garea + s) : 0.0f;
-        float4 O = kMom ? make_float4(x0, y0, z0, 0.f) : J.org[w];
+        float4 O = kOrig ? make_float4(x0, y0, z0, 0.f) : J.org[w];
         if (x < -Lx / 2) {
           x += Lx; O.x += Lx;
           if (MODE & NZ_MODE_PHI) kahan_add(fx, kx, Lx * Ga);
@@ -289,11 +291,18 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
           z -= Lz; O.z -= Lz;
           if (MODE & NZ_MODE_PHI) kahan_add(fz, kz, -(Lz * Ga));
         }
-        if (kMom) {
+        if (kOrig) {
           x0 = O.x; y0 = O.y; z0 = O.z;
         } else {
           J.org[w] = O;
         }
+      }
+      if (kDisp) {  // coalesced across the warp's walkers of one step
+        const size_t N = size_t(J.nwalkers);
+        float* d = J.disp + size_t(s - s0) * 3 * N;
+        d[w] = x - x0;
+        d[N + w] = y - y0;
+        d[2 * N + w] = z - z0;
       }
       if (kMom) {
         const float ex = x - x0, ey = y - y0, ez = z - z0;
@@ -323,7 +332,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     if (s < s1) jump_of(J, wid, next_step, next_draw, ds, jx, jy, jz);
   }
   J.pos[w] = make_float4(x, y, z, __int_as_float(label));
-  if (kMom) J.org[w] = make_float4(x0, y0, z0, __uint_as_float(wid));
+  if (kOrig) J.org[w] = make_float4(x0, y0, z0, __uint_as_float(wid));
   if (MODE & (NZ_MODE_PHI | NZ_MODE_SIG)) J.phi[w] = make_float4(fx, fy, fz, sig);
   if (MODE & NZ_MODE_PHI) {
     float4* c = J.comp + w;
@@ -474,6 +483,7 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
   j.phi = reinterpret_cast<float4*>(st.phi);
   j.comp = reinterpret_cast<float4*>(st.comp);
   j.moments = moments;
+  j.disp = nullptr;
   return j;
 }
 
@@ -496,7 +506,7 @@ void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items,
 // jobs == null: the single job `single` with n_items CTAs of kFusedThreads walkers.
 int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
                  int step1, int* queue, int grid, int threads, cudaStream_t st) {
-  switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS | NZ_MODE_TANGENT64)) {
+  switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS | NZ_MODE_TANGENT64 | kModeDisp)) {
     case NZ_MODE_PHI | NZ_MODE_TANGENT64:
       launch_mode<NZ_MODE_PHI | NZ_MODE_TANGENT64>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
       break;
@@ -512,6 +522,10 @@ int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_it
       launch_mode<NZ_MODE_SIG | NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     case NZ_MODE_MOMENTS:
       launch_mode<NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
+    case NZ_MODE_SIG | kModeDisp:
+      launch_mode<NZ_MODE_SIG | kModeDisp>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
+    case kModeDisp:
+      launch_mode<kModeDisp>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     case 0: launch_mode<0>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
     default: return set_error(NZ_ERR_ARG, "fused walk: unsupported mode %d", mode);
   }

@@ -201,6 +201,30 @@ __global__ void __launch_bounds__(256) moments_kernel(const float* __restrict__ 
   }
 }
 
+// The moments of every step of a fused launch from the displacements it
+// stored: step blockIdx.y, walkers strided over blockIdx.x; each term is
+// moments_kernel's (float displacement, squared and summed in FP64).
+__global__ void __launch_bounds__(256) disp_moments_kernel(const float* __restrict__ disp, int N,
+                                                           double* __restrict__ out) {
+  __shared__ double s_red[32];
+  const float* d = disp + size_t(blockIdx.y) * 3 * size_t(N);
+  double m[6] = {0, 0, 0, 0, 0, 0};
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < N; w += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float v = d[size_t(a) * N + w];
+      const double v2 = double(v) * double(v);
+      m[a] += v2;
+      m[3 + a] += v2 * v2;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const double t = block_sum(m[i], s_red);
+    if (threadIdx.x == 0) atomicAdd(out + size_t(blockIdx.y) * 6 + i, t);
+  }
+}
+
 }  // namespace nz
 
 using namespace nz;

@@ -101,6 +101,7 @@ class DiffSim3d:
         self.set_block_grid(nspins)
         self.issetup = False
         self._sub = None
+        self._fsub = None
         self._step = 0
         self._key = None
 
@@ -133,6 +134,7 @@ class DiffSim3d:
         self.pars['D'] = ','.join(map(str, [s.D for s in geom.structures]))
         self.pars['T2'] = ','.join(map(str, [s.T2 for s in geom.structures]))
         self._sub = None
+        self._fsub = None
         self.issetup = False
 
     def set_block_grid(self, nspins):
@@ -159,6 +161,25 @@ class DiffSim3d:
             self.segments = np.zeros(0, np.intc)
         self.pars['nspheres_per_seg'] = self.spheres_per_segment
         self.issetup = False
+
+    # cell edge of the fused walk's own lists: 0.5 um (the fastest measured on
+    # packed beaded-axon substrates), coarser for boxes that would need more
+    # than about 4M cells
+    FUSED_CELL = 0.5
+    FUSED_NEAR_MARGIN = 0.5
+    FUSED_MAX_CELLS = 4_000_000
+
+    def _fused_substrate(self):
+        """Cell lists of the fused walk, built once per geometry.  They do not
+        depend on set_segments: nseg sets the reference's padded table and the
+        per-step path, while the fused walk scans its own finer grid.  The grid
+        changes which spheres a walker scans, never a trajectory (every list
+        holds every sphere within the 1 um margin the reference's lists hold)."""
+        if self._fsub is None:
+            vol = float(self.geom.Lx) * float(self.geom.Ly) * float(self.geom.Lz)
+            cell = max(self.FUSED_CELL, (vol / self.FUSED_MAX_CELLS) ** (1.0 / 3.0))
+            self._fsub = self.geom.device_substrate(cell=cell, near_margin=self.FUSED_NEAR_MARGIN)
+        return self._fsub
 
     # -- set-up (diffsim3d.py:35-63) ----------------------------------------
     def setup(self, structures=None, initstates_int=None):
@@ -230,11 +251,16 @@ class DiffSim3d:
             tgt[step_idx] += v.to(tgt.dtype)
 
     # -- fused: many steps per launch -------------------------------------------
-    def run_fused(self, G, Garea, dt, mode, steps_per_launch=500, coarsen=4, phi=None, moments=None):
+    def run_fused(self, G, Garea, dt, mode, steps_per_launch=2000, coarsen=None, phi=None, moments=None):
         """All steps of the G / Garea tables through the fused walk, on the
-        walkers of this object (positions, spins0, sig and Phi updated)."""
+        walkers of this object (positions, spins0, sig and Phi updated).
+        Walkers are re-binned between launches by (label, bin) with bins of
+        about 4 um (``coarsen`` cells per axis)."""
         if not self.issetup:
             self.setup()
+        fsub = self._fused_substrate()
+        if coarsen is None:
+            coarsen = max(1, int(round(4.0 / (float(self.geom.Lx) / fsub.nseg[0]))))
         G = torch.as_tensor(np.asarray(G, np.float32), device="cuda")
         Garea = torch.as_tensor(np.asarray(Garea, np.float32), device="cuda")
         n = int(G.numel())
@@ -246,17 +272,28 @@ class DiffSim3d:
         spare = engine.FusedState(self.nspins)
         scratch = None
         s0 = 0
-        per = steps_per_launch if not (mode & L.MODE_MOMENTS) else min(steps_per_launch, L.MOMENT_STEPS)
+        # moments without phase: the walk stores per-step displacements (at
+        # most about 1 GiB of them per launch) and one reduction forms the sums
+        disp = bool(mode & L.MODE_MOMENTS) and not (mode & (L.MODE_PHI | L.MODE_PHASE))
+        dscratch = None
+        if disp:
+            per = max(1, min(steps_per_launch, (1 << 30) // (12 * max(self.nspins, 1))))
+        else:
+            per = steps_per_launch if not (mode & L.MODE_MOMENTS) else min(steps_per_launch, L.MOMENT_STEPS)
         Gs = torch.zeros(self._step + n, dtype=torch.float32, device="cuda")
         Gas = torch.zeros_like(Gs)
         Gs[self._step:] = G
         Gas[self._step:] = Garea
         while s0 < n:
             s1 = min(n, s0 + per)
-            scratch = st.sort_into(spare, self._sub.grid, coarsen, scratch, nlabels=self._sub.nstructures + 1)
+            scratch = st.sort_into(spare, fsub.grid, coarsen, scratch, nlabels=fsub.nstructures + 1)
             st, spare = spare, st
-            engine.walk_fused(self._sub, st, mode, dt, Gs, Gas, self._step + s0, self._step + s1, self._draws,
-                              moments=moments)
+            if disp:
+                dscratch = engine.walk_fused_moments(fsub, st, mode & L.MODE_SIG, dt, self._step + s0,
+                                                     self._step + s1, self._draws, moments, dscratch)
+            else:
+                engine.walk_fused(fsub, st, mode, dt, Gs, Gas, self._step + s0, self._step + s1, self._draws,
+                                  moments=moments)
             s0 = s1
         st.to_walkers_by_id(wk)  # back to walker-id order, the reference's layout
         self._label = wk.label

@@ -364,5 +364,22 @@ def walk_fused(sub: DeviceSubstrate, st: FusedState, mode: int, dt: float, G: to
                                    int(step1), L.byref(draws), _p(moments), _stream()), "nz_walk_fused")
 
 
+def walk_fused_moments(sub: DeviceSubstrate, st: FusedState, mode: int, dt: float, step0: int, step1: int,
+                       draws: L.Draws, moments: torch.Tensor, scratch: torch.Tensor | None = None) -> torch.Tensor:
+    """Steps [step0, step1) with the per-step displacement moments added to
+    moments[step0:step1] ([nsteps, 6] float64).  Returns the scratch buffer
+    (float32, grown as needed) for reuse."""
+    lib = L.load()
+    need = int(lib.nz_walk_fused_moments_scratch_bytes(st.N, int(step1) - int(step0)))
+    if scratch is None or scratch.numel() * 4 < need:
+        scratch = torch.empty(max(need // 4, 1), dtype=torch.float32, device=_dev())
+    s = sub.struct()
+    a = st.struct()
+    L.check(lib.nz_walk_fused_moments(L.byref(s), L.byref(a), mode, np.float32(dt), None, None, int(step0),
+                                      int(step1), L.byref(draws), _p(scratch), scratch.numel() * 4, _p(moments),
+                                      _stream()), "nz_walk_fused_moments")
+    return scratch
+
+
 def moments(spins: torch.Tensor, spins0: torch.Tensor, out: torch.Tensor):
     L.check(L.load().nz_moments(_p(spins), _p(spins0), int(spins.shape[1]), _p(out), _stream()), "nz_moments")

@@ -46,6 +46,28 @@ def packed_workload():
     return sub, pg, dirs, np.array([0.0, 1.0, 2.0, 3.0])
 
 
+def calibration_substrate() -> Substrate:
+    """A stand-in for the reference's segment-calibration substrate
+    (VF0.65_d1.68_OD200_bead1.0_500axons, docs/2_calibration.md:98-108):
+    500 beaded axons, base diameter lognormal (mean 1.68 um, sd 0.45 um),
+    beads of +20-50 % radius every 5.7 um, spheres every 0.5 um, packed
+    parallel (no orientation dispersion) in a periodic 50 um cube to a
+    volume fraction of 0.65 (seed 7).  About a minute to pack; cached."""
+    from .substrates import packed_axons
+    CACHE.mkdir(parents=True, exist_ok=True)
+    path = CACHE / "calibration_500axons_v1.pkl"
+    if path.exists():
+        with open(path, "rb") as f:
+            return pickle.load(f)
+    s = packed_axons(n_axons=500, L=(50.0, 50.0, 50.0), spheres_per_axon=100, r_mean=0.84, r_sd=0.225,
+                     bead_amp=(0.2, 0.5), bead_spacing=5.7, r_min=0.3, seed=7, max_iter=3000)
+    tmp = path.with_suffix(".tmp")
+    with open(tmp, "wb") as f:
+        pickle.dump(s, f)
+    os.replace(tmp, path)
+    return s
+
+
 def bundle(n_axons: int, seed: int) -> Substrate:
     CACHE.mkdir(parents=True, exist_ok=True)
     key = hashlib.sha1(f"axon_bundle-v1-{n_axons}-{seed}".encode()).hexdigest()[:16]

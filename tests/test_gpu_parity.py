@@ -292,3 +292,63 @@ def test_fused_near_lists_match_full_lists(eng, name, margin):
     np.testing.assert_array_equal(wk.phi.cpu().numpy(), phi)
     np.testing.assert_array_equal(wk.label.cpu().numpy(), r["label"])
     np.testing.assert_array_equal(wk.flags.cpu().numpy(), r["flags"])
+
+
+def test_fused_moments_equal_per_step_moments(eng):
+    """Narrow-pulse moments accumulated inside the fused walk (lanes of a warp
+    in lock-step, warp shuffle sums) against the plain walk with one moment
+    reduction per step (computeDiffusionCoefficientsAndKurtosis's role,
+    sim3d_kernel.cu:162-238): identical trajectories, per-step sums equal to
+    float summation order.  3001 walkers leave partial warps; 300 steps span
+    two launches."""
+    from nozomi_b200 import _lib as L
+    from nozomi_b200.simulate import device_substrate
+    from nozomi_b200.substrates import axon_bundle
+    sub = axon_bundle(12, seed=3)
+    dsub = device_substrate(sub, D=2.0, cell=0.5, near_margin=0.5)
+    N, nt, dt = 3001, 300, 0.005
+    x0, lab = eng.seed(dsub, list(range(sub.nstructures + 1)), N, key=99)
+    draws = eng.philox_draws(4242)
+    # plain: one launch and one moment reduction per step
+    wk = eng.Walkers.with_counters(x0.clone(), x0.clone(), sig=torch.ones(N, device="cuda"))
+    per_step = torch.zeros((nt, 6), dtype=torch.float64, device="cuda")
+    for s in range(nt):
+        eng.walk_step(dsub, wk, L.MODE_SIG, dt, 0.0, 0.0, s, draws)
+        eng.moments(wk.spins, wk.spins0, per_step[s])
+    # fused: moments inside the walk, at most L.MOMENT_STEPS steps per launch
+    w2 = eng.Walkers(x0.clone(), x0.clone(), sig=torch.ones(N, device="cuda"), label=lab.clone(),
+                     phi=torch.zeros((6, N), device="cuda"))
+    st = eng.FusedState.from_walkers(w2)
+    fused = torch.zeros((nt, 6), dtype=torch.float64, device="cuda")
+    zeros = torch.zeros(nt, device="cuda")
+    for s0 in range(0, nt, L.MOMENT_STEPS):
+        eng.walk_fused(dsub, st, L.MODE_SIG | L.MODE_MOMENTS, dt, zeros, zeros, s0, min(nt, s0 + L.MOMENT_STEPS),
+                       draws, moments=fused)
+    out = eng.Walkers(torch.empty((3, N), device="cuda"), torch.empty((3, N), device="cuda"),
+                      sig=torch.empty(N, device="cuda"))
+    st.to_walkers_by_id(out)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.spins.cpu().numpy(), wk.spins.cpu().numpy())
+    np.testing.assert_array_equal(out.sig.cpu().numpy(), wk.sig.cpu().numpy())
+    np.testing.assert_allclose(fused.cpu().numpy(), per_step.cpu().numpy(), rtol=2e-5, atol=0)
+    # the displacement form (nz_walk_fused_moments): every term is nz_moments',
+    # so the sums agree to FP64 summation order; any number of steps per call
+    w3 = eng.Walkers(x0.clone(), x0.clone(), sig=torch.ones(N, device="cuda"), label=lab.clone(),
+                     phi=torch.zeros((6, N), device="cuda"))
+    st3 = eng.FusedState.from_walkers(w3)
+    disp = torch.zeros((nt, 6), dtype=torch.float64, device="cuda")
+    scratch = None
+    for s0, s1 in ((0, 7), (7, 300)):
+        scratch = eng.walk_fused_moments(dsub, st3, L.MODE_SIG, dt, s0, s1, draws, disp, scratch)
+    out3 = eng.Walkers(torch.empty((3, N), device="cuda"), torch.empty((3, N), device="cuda"),
+                       sig=torch.empty(N, device="cuda"))
+    st3.to_walkers_by_id(out3)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out3.spins.cpu().numpy(), wk.spins.cpu().numpy())
+    np.testing.assert_array_equal(out3.sig.cpu().numpy(), wk.sig.cpu().numpy())
+    np.testing.assert_allclose(disp.cpu().numpy(), per_step.cpu().numpy(), rtol=1e-12, atol=0)
+    with pytest.raises(eng.NozomiError):  # scratch too small
+        L.check(L.load().nz_walk_fused_moments(L.byref(dsub.struct()), L.byref(st3.struct()), 0, 0.005, None, None,
+                                               0, 10, L.byref(draws), scratch.data_ptr(), 16,
+                                               disp.data_ptr(), torch.cuda.current_stream().cuda_stream),
+                "nz_walk_fused_moments")
