@@ -308,8 +308,11 @@ def run_ours(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # a short collective timeout: a rank that died ends the others' next
+        # collective with an error instead of a hang (set-up before the first
+        # barrier takes well under this)
+        from nozomi_b200.shard import init_process_group
+        init_process_group("nccl", timeout_s=180)
     engine.require_cuda()
     sub, pg, dirs, bvals = workload()
     # launch shape tuned for this workload (profiles/walk_fused_packed_tuning.md):

@@ -168,6 +168,7 @@ class DiffSim3d:
     FUSED_CELL = 0.5
     FUSED_NEAR_MARGIN = 0.5
     FUSED_MAX_CELLS = 4_000_000
+    DISP_BUDGET = 1 << 30  # bytes of per-step displacements one moments launch may store
 
     def _fused_substrate(self):
         """Cell lists of the fused walk, built once per geometry.  They do not
@@ -277,7 +278,7 @@ class DiffSim3d:
         disp = bool(mode & L.MODE_MOMENTS) and not (mode & (L.MODE_PHI | L.MODE_PHASE))
         dscratch = None
         if disp:
-            per = max(1, min(steps_per_launch, (1 << 30) // (12 * max(self.nspins, 1))))
+            per = max(1, min(steps_per_launch, self.DISP_BUDGET // (12 * max(self.nspins, 1))))
         else:
             per = steps_per_launch if not (mode & L.MODE_MOMENTS) else min(steps_per_launch, L.MOMENT_STEPS)
         Gs = torch.zeros(self._step + n, dtype=torch.float32, device="cuda")

@@ -57,6 +57,21 @@ def test_cells_match_oracle(eng):
         np.testing.assert_array_equal(seg.cpu().numpy(), seg_ref)
 
 
+def test_padded_table_full_size(eng):
+    """The reference's padded table built on the GPU (nz_segments_fill) for
+    the packed workload's 29,628 spheres on 40x40x80 cells (K = 45) against
+    the oracle's C restatement of set_segments."""
+    from nozomi_b200.substrates import cell_grid
+    from nozomi_b200.workloads import packed_workload
+    sub = packed_workload()[0]
+    nseg = cell_grid(sub.L, 1.0)
+    dsub = eng.DeviceSubstrate(sub.spheres(), sub.nstructures, sub.L, nseg, np.full(sub.nstructures + 1, 2.0),
+                               np.full(sub.nstructures + 1, 100.0))
+    K, seg = dsub.padded_segments()
+    assert K == int(oz.cells(sub.spheres(), sub.L, nseg)[1].max())
+    np.testing.assert_array_equal(seg.cpu().numpy(), oz.segments(sub.spheres(), sub.L, nseg, K))
+
+
 @pytest.mark.parametrize("name", NARROW)
 def test_plain_narrow_matches_reference(eng, name):
     c = load(name)
