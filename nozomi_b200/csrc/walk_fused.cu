@@ -13,14 +13,22 @@
 //    pass proves that label (some containing sphere of that structure, none of
 //    a lower one) or the iteration is redone with the recomputed label, so the
 //    result is the reference's;
-//  * a sphere whose (r + tol) ball lies more than 2 % + 2 nm beyond this
-//    iteration's reach |j| * jump_remaining cannot lower the jump fraction
-//    (its root exceeds jump_remaining), so its quadratic is skipped; the
-//    remaining candidates are collected in a 32-bit mask per 32-sphere chunk
-//    and solved afterwards, so a warp pays for the most candidates of any lane
-//    rather than for the union of all lanes' candidates;
+//  * the list is scanned in two passes.  The first, predicated and over
+//    every entry, marks the near spheres: a sphere whose (r + tol) ball lies
+//    more than 2 % + 2 nm beyond this iteration's reach |j| * jump_remaining
+//    neither contains the walker nor can lower the jump fraction (its root
+//    exceeds jump_remaining), so it is dropped.  The second, over the near
+//    spheres of a 32-entry chunk only, runs the reference's inside test and
+//    the fractions, so a warp pays for the most near spheres of any lane
+//    rather than for every entry twice;
+//  * the near lists (the same cell grid with a smaller margin) serve every
+//    iteration whose reach fits their margin; the full lists the rest;
 //  * the cell list entries carry their sphere's (cx, cy, cz, r) and structure
-//    id inline (one 16-byte and one 4-byte read-only load per entry);
+//    id inline (one 16-byte and one 4-byte read-only load per entry; walkers
+//    in the box read no structure id);
+//  * each iteration has one draw site (the scatter draw of this step or the
+//    first draw of the next), and the inside and outside fractions share one
+//    instruction stream (step_either);
 //  * phase is accrued as the 3-vector Phi = sum_n G_n p_n with Kahan
 //    compensation, the wrap correction on the wrapped axis only; every
 //    direction's phase is u_d . Phi (the reference's per-direction sums
