@@ -131,3 +131,40 @@ def test_precision_study_single_axon():
         assert report[name]["walk_max_err_in_sigma"] <= 4.0, name
         assert float(np.abs(res[name][0] - S64)[:, 0].max()) < 1e-12  # |G| = 0: no phase
     assert report["kahan"]["accrual_max_err"] <= 1e-5
+
+
+def test_phase_accrual_packed_workload():
+    """Phase accrual on the headline workload: 20,000 walkers of the packed
+    substrate through all 6000 steps, 30 directions x 4 b.  The fused walk
+    (Kahan Phi) against the exact FP64 phase of the same FP32 trajectories
+    from the oracle: positions bit for bit, signal within 1e-5 (the Kahan
+    bar; the north-star bar is 1e-3)."""
+    from nozomi_b200 import engine
+    from nozomi_b200.simulate import DwiRun, Tuning, device_substrate
+    from nozomi_b200.waveforms import step_tables
+    from nozomi_b200.workloads import packed_workload
+    from oracle import oracle as oz
+    sub, pg, dirs, bvals = packed_workload()
+    amps = pg.amplitude_for_b(bvals)
+    tuning = Tuning(cell=0.5, near_margin=0.5, coarsen=8, steps_per_launch=2000)
+    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin)
+    N, key = 20_000, 1000
+    run = DwiRun(dsub, pg, dirs, amps, N, seed=key, tuning=tuning)
+    x0, lab0 = run.initial_positions()
+    run.prepare(x0, lab0).walk()
+    S = run.signal()
+    spins_gpu = run.walkers().spins.cpu().numpy()
+    g = oz.Geometry(dsub.spheres.cpu().numpy(), dsub.nstructures, dsub.L, dsub.nseg, dsub.cell_start.cpu().numpy(),
+                    dsub.cell_count.cpu().numpy(), dsub.cell_items.cpu().numpy()[:dsub.n_items], dsub.D.cpu().numpy(),
+                    dsub.T2.cpu().numpy())
+    G, Ga = step_tables(pg)
+    xn = x0.cpu().numpy()
+    sp, s0, phi = xn.copy(), xn.copy(), np.zeros((6, N), np.float32)
+    ph64 = np.zeros((dirs.shape[1], N))
+    oz.walk_f32(g, oz.philox(key), oz.MODE_PHI, sp, s0, 0, G.size, pg.dt, G=G, Garea=Ga, phi=phi,
+                diffdir=dirs.astype(np.float32), phase64=ph64, counters=False)
+    np.testing.assert_array_equal(spins_gpu, sp)
+    exact = oz.signal_phase(ph64, np.asarray(amps, np.float64))
+    err = float(np.abs(S - exact).max())
+    print("packed accrual max err", err)
+    assert err <= 1e-5, err
