@@ -540,9 +540,19 @@ def run_batched(args):
     from nozomi_b200.plain import run_plain
     from nozomi_b200.simulate import Tuning
     from nozomi_b200.workloads import mixed_specs
+    import torch.distributed as dist
+    from nozomi_b200.shard import init_process_group, shard_jobs
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        init_process_group("nccl", timeout_s=180)
     engine.require_cuda()
-    specs = mixed_specs(seed=4, n_jobs=args.jobs, walker_scale=args.walker_scale)
+    all_specs = mixed_specs(seed=4, n_jobs=args.jobs, walker_scale=args.walker_scale)
+    # over several GPUs the jobs shard whole, longest first onto the least
+    # loaded rank; no data crosses ranks
+    mine = shard_jobs([sp.walker_steps for sp in all_specs], world)[rank] if world > 1 else range(len(all_specs))
+    specs = [all_specs[i] for i in mine]
     tuning = Tuning()
     if args.steps_per_launch:
         tuning.steps_per_launch = args.steps_per_launch
@@ -575,9 +585,28 @@ def run_batched(args):
         torch.cuda.synchronize()
         ms += e0.elapsed_time(e1)
     clk = clocks.stop()
-    ws = run.walker_steps()
+    del graph
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
+    ws = sum(sp.walker_steps for sp in all_specs)
     value = ws * args.steps / (ms * 1e-3)
     sig_batched = run.signals()
+    if world > 1:  # the plain comparison is a one-GPU measurement
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                              "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                              "data": "synthetic (seeded substrates, protocols and walkers)",
+                              "config": {"workload": BATCH_WORKLOAD.format(jobs=len(all_specs),
+                                                                           scale=args.walker_scale),
+                                         "jobs": len(all_specs), "walker_steps_per_step": ws,
+                                         "parallelism": f"jobs sharded whole over {world} GPUs"},
+                              "clocks": clk}), flush=True)
+        return 0
     # the plain per-substrate path, one job after another, launched from the
     # host, on cell lists of the default shape (1 um cells; not the batch's
     # tuned shape, which the plain kernel does not benefit from)
@@ -624,6 +653,8 @@ def run_batched(args):
 
 def run_serving(args):
     import torch
+    if int(os.environ.get("RANK", "0")) != 0:  # a one-GPU request loop
+        return 0
     from nozomi_b200 import engine
     from nozomi_b200.batch import SubstrateCache
     from nozomi_b200.plain import run_plain
