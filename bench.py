@@ -77,6 +77,8 @@ def parse():
                          "narrow: the narrow-pulse simulation CLI path on a calibration-like substrate")
     ap.add_argument("--rates", default="5,20,50,100,200", help="serving: request rates (req/s)")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="serving: arrival window per rate")
+    ap.add_argument("--serve-cell", type=float, default=1.5, help="serving: cell edge of the cached lists, um")
+    ap.add_argument("--serve-coarsen", type=int, default=8, help="serving: re-binning bins in cells per axis")
     ap.add_argument("--max-requests", type=int, default=200, help="serving: requests per rate at most")
     ap.add_argument("--jobs", type=int, default=64, help="batched: number of substrates")
     ap.add_argument("--walker-scale", type=float, default=1.0, help="batched: scale of the walker counts")
@@ -663,7 +665,9 @@ def run_serving(args):
     from nozomi_b200.workloads import request_stream
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     engine.require_cuda()
-    tuning = Tuning()
+    # the cell lists and re-binning of the autotuner's choice for this
+    # substrate distribution (1.5 um cells, 12 um bins); a round is 500 steps
+    tuning = Tuning(cell=args.serve_cell, coarsen=args.serve_coarsen, steps_per_launch=500)
     if args.steps_per_launch:
         tuning.steps_per_launch = args.steps_per_launch
     cache = SubstrateCache()
@@ -686,13 +690,15 @@ def run_serving(args):
         per_rate.append(st)
         all_done += done
     clk = clocks.stop()
-    # the plain per-substrate kernel on a sample of the same requests, one after another
+    # the plain per-substrate kernel on a sample of the same requests, one
+    # after another, on cell lists of the default shape (1 um cells)
     sample = all_done[:: max(1, len(all_done) // 8)][:8]
     stream = torch.cuda.current_stream()
     pms, pws = 0.0, 0
+    plain_cache = SubstrateCache()
     for t in sample:
         sp = t.spec
-        dsub = cache.get(sp.key, sp.substrate, sp.D, sp.T2, tuning)
+        dsub = plain_cache.get(sp.key, sp.substrate, sp.D, sp.T2, Tuning())
         x, _ = engine.seed(dsub, list(range(dsub.nstructures + 1)), sp.N, key=sp.seed ^ 0x5EED)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -713,7 +719,8 @@ def run_serving(args):
                                    "with probability 0.7, 1e4-5e5 walkers, 2000-8000 steps at 5 us, 6-60 directions, "
                                    "b<=3 ms/um^2, seed 5", "rates": args.rates,
                        "arrival_window_s": args.serve_seconds, "max_requests_per_rate": args.max_requests,
-                       "steps_per_launch": tuning.steps_per_launch, "threads": args.threads},
+                       "steps_per_launch": tuning.steps_per_launch, "threads": args.threads,
+                       "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen},
             "per_rate": per_rate,
             "plain": {"value": plain_value, "unit": "walker-steps/s", "requests_timed": len(sample),
                       "launch": "one plain-kernel launch per step, requests one after another"},
