@@ -272,20 +272,21 @@ __global__ void gather_records_kernel(const float* __restrict__ spheres, int S, 
   sph4[k] = make_float4(spheres[s], spheres[S + s], spheres[2 * S + s], spheres[3 * S + s]);
 }
 
-// Single-CTA exclusive scan (1024 threads, 8 items per thread per pass).
-__global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ in, int* __restrict__ out, int n,
-                                                    int* __restrict__ total) {
+// Exclusive scan of in[lo, hi) into out[lo, hi) by one CTA (1024 threads, 8
+// items per thread per pass), starting from carry; returns the range's total
+// (in every thread).
+__device__ __forceinline__ int block_scan_range(const int* __restrict__ in, int* __restrict__ out, int lo, int hi,
+                                                int carry) {
   constexpr int kItems = 8;
   __shared__ int s_warp[32];
-  int carry = 0;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int base = 0; base < n; base += 1024 * kItems) {
+  for (int base = lo; base < hi; base += 1024 * kItems) {
     int v[kItems];
     int sum = 0;
     const int first = base + threadIdx.x * kItems;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-      v[j] = (first + j < n) ? in[first + j] : 0;
+      v[j] = (first + j < hi) ? in[first + j] : 0;
       sum += v[j];
     }
     int x = sum;
@@ -309,13 +310,63 @@ __global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ in, 
     int run = carry + (wid > 0 ? s_warp[wid - 1] : 0) + x - sum;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-      if (first + j < n) out[first + j] = run;
+      if (first + j < hi) out[first + j] = run;
       run += v[j];
     }
     carry += s_warp[31];
     __syncthreads();
   }
-  if (threadIdx.x == 0 && total) *total = carry;
+  return carry;
+}
+
+// Single-CTA exclusive scan of n ints.
+__global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ in, int* __restrict__ out, int n,
+                                                    int* __restrict__ total) {
+  const int t = block_scan_range(in, out, 0, n, 0);
+  if (threadIdx.x == 0 && total) *total = t;
+}
+
+// Multi-CTA form for long arrays: each CTA sums one tile, one CTA scans the
+// tile sums, each CTA then scans its tile from its offset.
+__global__ void __launch_bounds__(1024) tile_sum_kernel(const int* __restrict__ in, int n, int* __restrict__ sums) {
+  __shared__ int s_red[32];
+  const int lo = blockIdx.x * kScanTile, hi = min(n, lo + kScanTile);
+  int v = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) v += in[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = s_red[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) sums[blockIdx.x] = v;
+  }
+}
+
+__global__ void __launch_bounds__(1024) tile_scan_kernel(const int* __restrict__ in, int* __restrict__ out, int n,
+                                                         const int* __restrict__ offsets) {
+  const int lo = blockIdx.x * kScanTile, hi = min(n, lo + kScanTile);
+  block_scan_range(in, out, lo, hi, offsets[blockIdx.x]);
+}
+
+int scan_tiles(int n) { return (n + kScanTile - 1) / kScanTile; }
+
+int exclusive_scan(const int* in, int* out, int n, int* tile_sums, int* tile_offsets, cudaStream_t st) {
+  if (n <= kScanSingle || !tile_sums || !tile_offsets) {
+    scan_kernel<<<1, 1024, 0, st>>>(in, out, n, nullptr);
+    return check_launch("scan_kernel");
+  }
+  const int tiles = scan_tiles(n);
+  tile_sum_kernel<<<tiles, 1024, 0, st>>>(in, n, tile_sums);
+  int rc = check_launch("tile_sum_kernel");
+  if (rc) return rc;
+  scan_kernel<<<1, 1024, 0, st>>>(tile_sums, tile_offsets, tiles, nullptr);
+  rc = check_launch("scan_kernel");
+  if (rc) return rc;
+  tile_scan_kernel<<<tiles, 1024, 0, st>>>(in, out, n, tile_offsets);
+  return check_launch("tile_scan_kernel");
 }
 
 }  // namespace nz

@@ -96,5 +96,12 @@ __global__ void unpack_kernel(nz_state st, nz_walkers wk, int by_id, int* bad);
 
 // ---- cells.cu ----
 __global__ void scan_kernel(const int* __restrict__ in, int* __restrict__ out, int n, int* __restrict__ total);
+// Exclusive scan of n ints on stream st: one CTA up to kScanSingle ints,
+// beyond that (with tile_sums and tile_offsets of scan_tiles(n) ints each)
+// one CTA per kScanTile ints.
+constexpr int kScanTile = 8192;
+constexpr int kScanSingle = 32768;
+int scan_tiles(int n);
+int exclusive_scan(const int* in, int* out, int n, int* tile_sums, int* tile_offsets, cudaStream_t st);
 
 }  // namespace nz

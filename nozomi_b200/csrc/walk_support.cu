@@ -252,7 +252,8 @@ static inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 extern "C" size_t nz_sort_scratch_bytes(int N, int nbins) {
   if (N < 0 || nbins < 0) return 0;
-  return align256(size_t(N) * sizeof(int)) + 2 * align256(size_t(nbins) * sizeof(int));
+  return align256(size_t(N) * sizeof(int)) + 2 * align256(size_t(nbins) * sizeof(int)) +
+         2 * align256(size_t(scan_tiles(nbins)) * sizeof(int));
 }
 
 extern "C" int nz_state_sort_keyed(const nz_state* in, const nz_grid* grid, int coarsen, int nlabels, nz_state* out,
@@ -278,13 +279,15 @@ extern "C" int nz_state_sort_keyed(const nz_state* in, const nz_grid* grid, int 
   int* bins = reinterpret_cast<int*>(p);
   int* hist = reinterpret_cast<int*>(p + align256(size_t(N) * sizeof(int)));
   int* cursor = reinterpret_cast<int*>(p + align256(size_t(N) * sizeof(int)) + align256(size_t(nbins) * sizeof(int)));
+  int* tile_sums = reinterpret_cast<int*>(reinterpret_cast<char*>(cursor) + align256(size_t(nbins) * sizeof(int)));
+  int* tile_offsets = reinterpret_cast<int*>(reinterpret_cast<char*>(tile_sums) +
+                                             align256(size_t(scan_tiles(int(nbins))) * sizeof(int)));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(hist, 0, size_t(nbins) * sizeof(int), st) != cudaSuccess) return check_launch("sort memset");
   bin_count_kernel<<<(N + 255) / 256, 256, 0, st>>>(reinterpret_cast<const float4*>(in->pos), N, b, bins, hist);
   int rc = check_launch("bin_count_kernel");
   if (rc) return rc;
-  scan_kernel<<<1, 1024, 0, st>>>(hist, cursor, int(nbins), nullptr);
-  rc = check_launch("scan_kernel");
+  rc = exclusive_scan(hist, cursor, int(nbins), tile_sums, tile_offsets, st);
   if (rc) return rc;
   bin_scatter_kernel<<<(N + 255) / 256, 256, 0, st>>>(*in, N, bins, cursor, *out);
   return check_launch("bin_scatter_kernel");

@@ -367,3 +367,39 @@ def test_fused_moments_equal_per_step_moments(eng):
                                                0, 10, L.byref(draws), scratch.data_ptr(), 16,
                                                disp.data_ptr(), torch.cuda.current_stream().cuda_stream),
                 "nz_walk_fused_moments")
+
+
+def test_sort_with_many_bins(eng):
+    """Re-binning with more bins than one CTA scans (128,000 bins: the
+    multi-CTA scan) and with labels (3 x 128,000 keys): the output is the
+    input's walkers, each record intact, in non-decreasing key order."""
+    rng = np.random.default_rng(21)
+    N = 250_000
+    pos = np.stack([rng.uniform(-20, 20, N), rng.uniform(-20, 20, N), rng.uniform(-40, 40, N)]).astype(np.float32)
+    lab = rng.integers(0, 3, N).astype(np.int32)
+    x = _dev(pos)
+    wk = eng.Walkers(x, x + 0.25, phi=_dev(rng.normal(0, 1, (6, N)).astype(np.float32)), label=_dev(lab))
+    src = eng.FusedState.from_walkers(wk)
+    grid = eng.box_grid((40.0, 40.0, 80.0), (40, 40, 80))
+
+    def canon(st):
+        p = st.pos.cpu().numpy()
+        ids = st.org.cpu().numpy()[:, 3].view(np.int32)
+        ix = np.clip(np.floor((p[:, 0] + 20.0) / 1.0), 0, 39).astype(np.int64)
+        iy = np.clip(np.floor((p[:, 1] + 20.0) / 1.0), 0, 39).astype(np.int64)
+        iz = np.clip(np.floor((p[:, 2] + 40.0) / 1.0), 0, 79).astype(np.int64)
+        cell = (iz * 40 + iy) * 40 + ix
+        order = np.argsort(ids)
+        rec = np.concatenate([getattr(st, t).cpu().numpy()[order] for t in ("pos", "org", "phi", "comp")], axis=1)
+        return cell, p[:, 3].view(np.int32), ids, rec
+
+    _, _, ids0, rec0 = canon(src)
+    for nlabels in (0, 3):
+        out = eng.FusedState(N)
+        src.sort_into(out, grid, 1, nlabels=nlabels)
+        torch.cuda.synchronize()
+        cell, label, ids, rec = canon(out)
+        np.testing.assert_array_equal(np.sort(ids), np.arange(N))
+        np.testing.assert_array_equal(rec, rec0)
+        key = cell if nlabels == 0 else label.astype(np.int64) * 128000 + cell  # label * bins + bin
+        assert np.all(np.diff(key) >= 0)
