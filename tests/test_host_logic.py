@@ -1,0 +1,71 @@
+"""Host logic that needs no GPU: the synthetic workload generators (seeded,
+within their stated ranges), the serving loop's memory footprint and latency
+statistics, and the autotuner's workload signature."""
+import numpy as np
+import pytest
+
+pytest.importorskip("torch")
+
+
+def _small_specs(seed=4, n=5):
+    from nozomi_b200.workloads import mixed_specs
+    return mixed_specs(seed=seed, n_jobs=n, axons=(10, 14), walkers=(1e4, 1e5), steps=(2000, 3000))
+
+
+def test_mixed_specs_seeded_and_in_range():
+    a, b = _small_specs(), _small_specs()
+    for x, y in zip(a, b):
+        assert (x.N, x.nsteps, x.seed, x.key) == (y.N, y.nsteps, y.seed, y.key)
+        np.testing.assert_array_equal(x.dirs, y.dirs)
+        assert 1e4 <= x.N <= 1e5 and x.N % 1000 == 0
+        assert 2000 <= x.nsteps <= 3000
+        assert 6 <= x.dirs.shape[1] <= 60
+        np.testing.assert_allclose(np.linalg.norm(x.dirs, axis=0), 1.0, atol=1e-12)
+        assert x.amplitudes[0] == 0.0 and np.all(np.diff(x.amplitudes) > 0)
+        assert 10 <= x.substrate.nstructures <= 14
+    assert [s.seed for s in _small_specs(seed=5)] != [s.seed for s in a]
+
+
+def test_request_stream_poisson_and_reuse():
+    from nozomi_b200.workloads import request_stream
+    reqs = request_stream(50.0, 4.0, seed=5, axons=(10, 12), walkers=(1e4, 2e4), steps=(2000, 2100))
+    t = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(t) > 0) and t[-1] <= 4.0
+    assert 120 <= len(reqs) <= 280  # 200 expected at 50 req/s over 4 s
+    keys = [r.spec.key for r in reqs]
+    reused = sum(1 for i, k in enumerate(keys) if k in keys[:i])
+    assert 0.5 < reused / len(keys) < 0.9  # substrates drawn again with probability 0.7
+    again = request_stream(50.0, 4.0, seed=5, axons=(10, 12), walkers=(1e4, 2e4), steps=(2000, 2100))
+    assert [r.arrival for r in again] == list(t) and [r.spec.N for r in again] == [r.spec.N for r in reqs]
+    capped = request_stream(50.0, 4.0, seed=5, axons=(10, 12), walkers=(1e4, 2e4), steps=(2000, 2100),
+                            max_requests=7)
+    assert len(capped) == 7
+
+
+def test_serving_footprint_and_latency_stats():
+    from nozomi_b200.serve import Ticket, footprint, latency_stats
+    from nozomi_b200.simulate import Tuning
+    specs = _small_specs(n=2)
+    small, big = sorted(specs, key=lambda s: s.N)
+    assert footprint(big, Tuning()) > footprint(small, Tuning()) > 2 * 64 * small.N
+    tickets = []
+    for i, lat in enumerate(np.linspace(0.1, 1.0, 100)):
+        t = Ticket(i, small, arrival=10.0)
+        t.completed = 10.0 + lat
+        tickets.append(t)
+    failed = Ticket(100, small, arrival=0.0)
+    failed.completed, failed.error = 50.0, "cancelled"
+    st = latency_stats(tickets + [failed])
+    assert st["n"] == 100
+    assert abs(st["p50_s"] - 0.55) < 1e-9 and abs(st["max_s"] - 1.0) < 1e-12
+    assert 0.98 < st["p99_s"] <= 1.0
+    assert latency_stats([failed]) == {"n": 0}
+
+
+def test_autotune_signature():
+    from nozomi_b200.autotune import signature
+    a = _small_specs()
+    assert signature(a) == signature(_small_specs())
+    b = _small_specs()
+    b[0] = __import__("dataclasses").replace(b[0], N=b[0].N * 50)
+    assert signature(b) != signature(a)
