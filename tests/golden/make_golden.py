@@ -3,9 +3,9 @@
 Run in a container that holds the reference tree (default /root/reference,
 override with NOZOMI_REFERENCE_ROOT):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [ingestion]
 
-The reference's own Python engine (DiffSim3d / DwiSim3d / SimGeometry3D,
+(``ingestion`` regenerates only tests/golden/ingestion.npz.)  The reference's own Python engine (DiffSim3d / DwiSim3d / SimGeometry3D,
 simulation_toolkit/simulation_engine/) is imported with a host stand-in for
 pycuda (oracle/fake_pycuda.py); its ``SourceModule`` compiles the reference's
 own template-substituted kernel source (sim3d_kernel.cu) for the CPU.  Draws are
@@ -226,8 +226,56 @@ def seeding_case(geo):
     print("wrote seeding")
 
 
+def ingestion_case(ag, tmpdir):
+    """The simulation driver's substrate ingestion (simulation_main.py:37-49):
+    the pickle read by common_utils.import_array_geometry_full_path, split at
+    z == L/2 by split_matrix_to_list, z-padded by createBoundaryZ.  Fibres run
+    from z = -L/2 to L/2; some continue through the z face as another fibre
+    (a tilted chain A -> B -> C -> A), some as themselves, one has no partner."""
+    import pickle
+    import torch
+    import simulation_toolkit.toolkit_params as params
+    import simulation_toolkit.utils.common_utils as cu
+    rng = np.random.default_rng(31)
+    L = 20.0
+    fibres = []
+    pts = [(-6.0, -4.0), (-3.0, 1.0), (2.0, 5.0)]  # the chain's entry points
+    for i, (a, b) in enumerate(zip(pts, pts[1:] + pts[:1])):  # A -> B -> C -> A
+        fibres.append((a, b))
+    fibres.append(((5.0, -5.0), (5.0, -5.0)))  # its own partner
+    fibres.append(((8.0, 8.0), (7.5, 8.5)))    # no fibre starts at (7.5, 8.5)
+    rows = []
+    for fid, ((x0, y0), (x1, y1)) in enumerate(fibres):
+        n = int(rng.integers(45, 70))
+        t = np.linspace(0.0, 1.0, n)
+        z = -L / 2 + t * L
+        z[-1] = L / 2  # the split marker: exactly L/2
+        x, y = x0 + t * (x1 - x0), y0 + t * (y1 - y0)
+        x[-1], y[-1] = x1, y1
+        r = rng.uniform(0.4, 1.2, n)
+        rows.append(np.stack([x, y, z, r, np.full(n, float(fid))], axis=1))
+    A = np.concatenate(rows)
+    path = Path(tmpdir) / "substrate.pkl"
+    with open(path, "wb") as f:
+        pickle.dump([torch.from_numpy(A), L], f, protocol=pickle.HIGHEST_PROTOCOL)
+    arr, Lr = cu.import_array_geometry_full_path(str(path))
+    params.BOX_LENGTH = Lr
+    fl = cu.split_matrix_to_list(arr)
+    out = ag.createBoundaryZ(fl, Lr)
+    np.savez_compressed(OUT / "ingestion.npz", matrix=A, L=L, lengths=np.array([len(f) for f in out]),
+                        fibres=np.concatenate(out))
+
+
 def main():
     ds3, geo, wf, ag = _load_reference()
+    if sys.argv[1:] == ["ingestion"]:
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            ingestion_case(ag, d)
+        return
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        ingestion_case(ag, d)
     segments_cases(ds3, geo)
     waveform_cases(wf)
     seeding_case(geo)

@@ -68,3 +68,25 @@ def test_cli_end_to_end(tmp_path):
     assert res["phase"].shape == (2, 5000)
     S = res["signal"].real
     assert S[0, 0] == pytest.approx(1.0) and S[1, -1] < S[0, -1]  # along the fibres attenuates more
+
+
+def test_ingestion_matches_reference_driver(tmp_path):
+    """Substrate ingestion against the reference's own code
+    (tests/golden/ingestion.npz, made by make_golden.py: the pickle read by
+    import_array_geometry_full_path, split at z == L/2, z-padded by
+    createBoundaryZ), on fibres that continue through the z face as another
+    fibre, as themselves, or not at all: every sphere, bit for bit."""
+    from tests._fixtures import GOLDEN
+    z = np.load(GOLDEN / "ingestion.npz")
+    A, L = z["matrix"], float(z["L"])
+    ref = np.split(z["fibres"], np.cumsum(z["lengths"])[:-1])
+    mine = sb.bound_z(sb.split_fibers(A.copy(), L), L)
+    assert len(mine) == len(ref)
+    for a, b in zip(mine, ref):
+        np.testing.assert_array_equal(a, b)
+    path = tmp_path / "s.pkl"
+    sb.save_pickle(path, A, L)
+    s = sb.from_pickle(path)
+    assert s.L == (L, L, L) and s.nstructures == len(ref)
+    for a, b in zip(s.fibers, ref):
+        np.testing.assert_array_equal(a, b[:, :4])
