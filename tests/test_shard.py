@@ -181,3 +181,17 @@ def test_sharded_gpu_equals_unsharded():
             pos.append(sh.run.walkers().spins.cpu().numpy())
         np.testing.assert_array_equal(np.concatenate(pos, axis=1), ref_pos)
         np.testing.assert_allclose((sums[0] + 1j * sums[1]) / N, ref_sig, rtol=0, atol=1e-12)
+
+
+def test_oracle_seed_range_is_a_slice_of_the_full_seeding():
+    """Walkers [id0, id0 + n) seeded alone are walkers id0.. of one seeding of
+    the whole run (positions and labels), the property sharded runs rest on."""
+    from oracle import oracle as oz
+    g = _oracle_problem()[0]
+    full, lab, left = oz.seed(g, [0, 1], 900, 4321)
+    assert left == 0
+    for id0, n in ((0, 300), (300, 250), (550, 350)):
+        part, plab, pleft = oz.seed(g, [0, 1], n, 4321, id0=id0)
+        assert pleft == 0
+        np.testing.assert_array_equal(part, full[:, id0:id0 + n])
+        np.testing.assert_array_equal(plab, lab[id0:id0 + n])
