@@ -19,7 +19,7 @@ from pathlib import Path
 import numpy as np
 import torch
 
-from .batch import BatchRun, JobSpec, SubstrateCache
+from .batch import BatchRun, SubstrateCache
 from .simulate import Tuning
 from .waveforms import ArbitraryWaveform
 

@@ -16,7 +16,7 @@ sample (diffsim3d.py:246-261).  Here every job of a batch advances together:
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 import torch
