@@ -286,12 +286,19 @@ class Clocks:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.f.close()
-        rows = [r.split(", ") for r in self.path.read_text().strip().splitlines() if r.strip()]
+        text = self.path.read_text()
         self.path.unlink(missing_ok=True)
+        return self.summarise(text)
+
+    @staticmethod
+    def summarise(text):
+        """Median SM clock, the maximum and the throttle reasons seen in
+        nvidia-smi's csv,noheader,nounits lines (the query of start())."""
+        rows = [r.split(", ") for r in text.strip().splitlines() if r.strip()]
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
+        sm = [float(r[1]) for r in rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        mx = float(rows[0][2]) if len(rows[0]) > 2 and rows[0][2].replace(".", "").isdigit() else None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and r[5 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
