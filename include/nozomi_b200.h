@@ -235,7 +235,10 @@ int nz_walk_fused_moments(const nz_substrate* sub, const nz_state* st, int mode,
  * device arrays; every job of one launch has mode `mode`.  grid = CTA count
  * (0 = one CTA per item, no queue); threads = walkers per CTA (a multiple of
  * 32 up to 256); an item holds at most `threads` walkers.  The batched form of
- * the fused walk: many substrates, protocols and walker sets in one launch. */
+ * the fused walk: many substrates, protocols and walker sets in one launch.
+ * The device arrays are not read back for checking: the caller guarantees
+ * 0 <= item.job < n_jobs, 1 <= item.count <= threads and
+ * item.first + item.count <= that job's state.N. */
 int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0, int step1,
                   int* queue, int grid, int threads, void* stream);
 

@@ -68,14 +68,17 @@ extern "C" int nz_walk_step(const nz_substrate* sub, const nz_walkers* wk, int m
                             int step, const nz_draws* draws, void* stream) {
   int rc = check_substrate(sub, "nz_walk_step");
   if (rc) return rc;
-  if (!wk || !draws || wk->N < 0 || !wk->spins || !wk->spins0 || !sub->cell_items || (sub->S > 0 && !sub->spheres))
+  if (!wk || !draws || wk->N < 0 || !sub->cell_items || (sub->S > 0 && !sub->spheres))
     return set_error(NZ_ERR_ARG, "nz_walk_step: bad walkers or draws");
-  if ((mode & NZ_MODE_PHASE) && (wk->ndir <= 0 || !wk->phase || !wk->diffdir))
-    return set_error(NZ_ERR_ARG, "nz_walk_step: phase mode needs phase and diffdir");
-  if ((mode & NZ_MODE_SIG) && (!wk->sig || !sub->T2)) return set_error(NZ_ERR_ARG, "nz_walk_step: sig mode needs sig, T2");
-  if ((mode & NZ_MODE_PHI) && !wk->phi) return set_error(NZ_ERR_ARG, "nz_walk_step: phi mode needs phi");
   if (mode & ~(NZ_MODE_SIG | NZ_MODE_PHASE | NZ_MODE_PHI)) return set_error(NZ_ERR_ARG, "nz_walk_step: mode %d", mode);
-  if (wk->N == 0) return NZ_OK;
+  if ((mode & NZ_MODE_PHASE) && wk->ndir <= 0) return set_error(NZ_ERR_ARG, "nz_walk_step: phase mode needs ndir > 0");
+  if ((mode & NZ_MODE_SIG) && !sub->T2) return set_error(NZ_ERR_ARG, "nz_walk_step: sig mode needs T2");
+  if (wk->N == 0) return NZ_OK;  // empty walker arrays may be null
+  if (!wk->spins || !wk->spins0) return set_error(NZ_ERR_ARG, "nz_walk_step: null spins or spins0");
+  if ((mode & NZ_MODE_PHASE) && (!wk->phase || !wk->diffdir))
+    return set_error(NZ_ERR_ARG, "nz_walk_step: phase mode needs phase and diffdir");
+  if ((mode & NZ_MODE_SIG) && !wk->sig) return set_error(NZ_ERR_ARG, "nz_walk_step: sig mode needs sig");
+  if ((mode & NZ_MODE_PHI) && !wk->phi) return set_error(NZ_ERR_ARG, "nz_walk_step: phi mode needs phi");
   PlainArgs a;
   a.g = to_grid(sub->grid);
   a.nstructures = sub->nstructures;
@@ -108,18 +111,25 @@ extern "C" int nz_walk_step(const nz_substrate* sub, const nz_walkers* wk, int m
   return check_launch("walk_plain_kernel");
 }
 
-static int check_state(const nz_state* st, const char* who) {
-  if (!st || st->N < 0 || !st->pos || !st->org || !st->phi || !st->comp)
-    return set_error(NZ_ERR_ARG, "%s: incomplete state", who);
+int nz::check_state(const nz_state* st, const char* who) {
+  if (!st || st->N < 0) return set_error(NZ_ERR_ARG, "%s: null state or negative N", who);
+  if (st->N == 0) return NZ_OK;
+  if (!st->pos || !st->org || !st->phi || !st->comp) return set_error(NZ_ERR_ARG, "%s: incomplete state", who);
   if (!aligned16(st->pos) || !aligned16(st->org) || !aligned16(st->phi) || !aligned16(st->comp))
     return set_error(NZ_ERR_ARG, "%s: state arrays must be 16-byte aligned", who);
+  return NZ_OK;
+}
+
+int nz::check_grid(const nz_grid* g, const char* who) {
+  if (!g || g->nx <= 0 || g->ny <= 0 || g->nz <= 0) return set_error(NZ_ERR_ARG, "%s: grid needs nx, ny, nz > 0", who);
   return NZ_OK;
 }
 
 extern "C" int nz_state_pack(const nz_walkers* wk, const uint32_t* walker_id, nz_state* st, void* stream) {
   int rc = check_state(st, "nz_state_pack");
   if (rc) return rc;
-  if (!wk || wk->N != st->N || !wk->spins || !wk->spins0) return set_error(NZ_ERR_ARG, "nz_state_pack: bad walkers");
+  if (!wk || wk->N != st->N || (st->N > 0 && (!wk->spins || !wk->spins0)))
+    return set_error(NZ_ERR_ARG, "nz_state_pack: bad walkers");
   if (st->N == 0) return NZ_OK;
   pack_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*wk, walker_id, *st);
   return check_launch("pack_kernel");
@@ -128,7 +138,8 @@ extern "C" int nz_state_pack(const nz_walkers* wk, const uint32_t* walker_id, nz
 extern "C" int nz_state_unpack(const nz_state* st, const nz_walkers* wk, void* stream) {
   int rc = check_state(st, "nz_state_unpack");
   if (rc) return rc;
-  if (!wk || wk->N != st->N || !wk->spins || !wk->spins0) return set_error(NZ_ERR_ARG, "nz_state_unpack: bad walkers");
+  if (!wk || wk->N != st->N || (st->N > 0 && (!wk->spins || !wk->spins0)))
+    return set_error(NZ_ERR_ARG, "nz_state_unpack: bad walkers");
   if (st->N == 0) return NZ_OK;
   unpack_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*st, *wk, 0, nullptr);
   return check_launch("unpack_kernel");
@@ -137,7 +148,7 @@ extern "C" int nz_state_unpack(const nz_state* st, const nz_walkers* wk, void* s
 extern "C" int nz_state_unpack_by_id(const nz_state* st, const nz_walkers* wk, int* n_bad, void* stream) {
   int rc = check_state(st, "nz_state_unpack_by_id");
   if (rc) return rc;
-  if (!wk || wk->N != st->N || !wk->spins || !wk->spins0)
+  if (!wk || wk->N != st->N || (st->N > 0 && (!wk->spins || !wk->spins0)))
     return set_error(NZ_ERR_ARG, "nz_state_unpack_by_id: bad walkers");
   if (st->N == 0) return NZ_OK;
   unpack_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*st, *wk, 1, n_bad);

@@ -428,6 +428,7 @@ extern "C" int nz_cells_gather(const float* spheres, int S, const int* items, in
     return set_error(NZ_ERR_ARG, "nz_cells_gather: bad arguments");
   if (reinterpret_cast<uintptr_t>(sph4) % 16 != 0) return set_error(NZ_ERR_ARG, "nz_cells_gather: sph4 not 16-byte aligned");
   if (n_items == 0) return NZ_OK;
+  if (ncell == 0) return set_error(NZ_ERR_ARG, "nz_cells_gather: %d items but no cells", n_items);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   float4* s4 = reinterpret_cast<float4*>(sph4);
   gather_ids_kernel<<<(n_items + 255) / 256, 256, 0, st>>>(spheres, S, items, n_items, s4, sid);

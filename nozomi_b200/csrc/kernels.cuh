@@ -8,6 +8,11 @@ namespace nz {
 
 int set_error(int status, const char* fmt, ...);
 int check_launch(const char* what);
+// Host-side argument checks shared by the entry points (capi.cu): a packed
+// state's four arrays present and 16-byte aligned (any, or none, when N is 0);
+// a grid with at least one cell per axis.
+int check_state(const nz_state* st, const char* who);
+int check_grid(const nz_grid* g, const char* who);
 
 // ---- plain walk (walk_plain.cu) ----
 struct PlainArgs {

@@ -232,8 +232,9 @@ using namespace nz;
 extern "C" int nz_seed_range(const nz_substrate* sub, const uint8_t* target, uint32_t id0, int N, uint32_t key0,
                              uint32_t key1, uint32_t stream_id, int max_rounds, float* spins, int* label,
                              int* n_unseeded, void* stream) {
-  if (!sub || !target || N < 0 || max_rounds <= 0 || !spins || !n_unseeded || !sub->cell_start || !sub->cell_count ||
-      !sub->cell_items || (sub->S > 0 && !sub->spheres) || uint64_t(id0) + uint64_t(N) > (uint64_t(1) << 32))
+  if (!sub || !target || N < 0 || max_rounds <= 0 || (N > 0 && !spins) || !n_unseeded || !sub->cell_start ||
+      !sub->cell_count || !sub->cell_items || (sub->S > 0 && !sub->spheres) ||
+      uint64_t(id0) + uint64_t(N) > (uint64_t(1) << 32))
     return set_error(NZ_ERR_ARG, "nz_seed_range: bad arguments");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(n_unseeded, 0, sizeof(int), st) != cudaSuccess) return check_launch("nz_seed memset");
@@ -258,8 +259,14 @@ extern "C" size_t nz_sort_scratch_bytes(int N, int nbins) {
 
 extern "C" int nz_state_sort_keyed(const nz_state* in, const nz_grid* grid, int coarsen, int nlabels, nz_state* out,
                                    void* scratch, size_t scratch_bytes, void* stream) {
-  if (!in || !grid || !out || coarsen <= 0 || nlabels < 0 || in->N != out->N || !scratch)
+  int rc = check_state(in, "nz_state_sort (in)");
+  if (rc == NZ_OK) rc = check_state(out, "nz_state_sort (out)");
+  if (rc == NZ_OK) rc = check_grid(grid, "nz_state_sort");
+  if (rc) return rc;
+  if (coarsen <= 0 || nlabels < 0 || in->N != out->N || !scratch)
     return set_error(NZ_ERR_ARG, "nz_state_sort: bad arguments");
+  if (in->N > 0 && (in->pos == out->pos || in->org == out->org || in->phi == out->phi || in->comp == out->comp))
+    return set_error(NZ_ERR_ARG, "nz_state_sort: in and out share an array (the sort is out of place)");
   BinGrid b;
   b.g = Grid{grid->Lx, grid->Ly, grid->Lz, grid->dLx, grid->dLy, grid->dLz, float(grid->nx), float(grid->ny),
              float(grid->nz)};
@@ -285,7 +292,7 @@ extern "C" int nz_state_sort_keyed(const nz_state* in, const nz_grid* grid, int 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(hist, 0, size_t(nbins) * sizeof(int), st) != cudaSuccess) return check_launch("sort memset");
   bin_count_kernel<<<(N + 255) / 256, 256, 0, st>>>(reinterpret_cast<const float4*>(in->pos), N, b, bins, hist);
-  int rc = check_launch("bin_count_kernel");
+  rc = check_launch("bin_count_kernel");
   if (rc) return rc;
   rc = exclusive_scan(hist, cursor, int(nbins), tile_sums, tile_offsets, st);
   if (rc) return rc;
@@ -300,7 +307,9 @@ extern "C" int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarse
 
 extern "C" int nz_signal_phi(const nz_state* st, const float* dirs, int ndir, const float* amp, int nb, double* out,
                              void* stream) {
-  if (!st || !dirs || !amp || !out || ndir <= 0 || nb <= 0) return set_error(NZ_ERR_ARG, "nz_signal_phi: bad arguments");
+  const int rc = check_state(st, "nz_signal_phi");
+  if (rc) return rc;
+  if (!dirs || !amp || !out || ndir <= 0 || nb <= 0) return set_error(NZ_ERR_ARG, "nz_signal_phi: bad arguments");
   if (st->N == 0) return NZ_OK;
   signal_kernel<<<(st->N + kSigThreads - 1) / kSigThreads, kSigThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       *st, dirs, ndir, amp, nb, out);
@@ -318,7 +327,9 @@ extern "C" int nz_signal_phase(const float* phase, int ndir, int N, const float*
 }
 
 extern "C" int nz_phase_from_phi(const nz_state* st, const float* dirs, int ndir, float* phase, void* stream) {
-  if (!st || !dirs || !phase || ndir <= 0) return set_error(NZ_ERR_ARG, "nz_phase_from_phi: bad arguments");
+  const int rc = check_state(st, "nz_phase_from_phi");
+  if (rc) return rc;
+  if (!dirs || (st->N > 0 && !phase) || ndir <= 0) return set_error(NZ_ERR_ARG, "nz_phase_from_phi: bad arguments");
   if (st->N == 0) return NZ_OK;
   phase_from_phi_kernel<<<(st->N + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(*st, dirs, ndir, phase);
   return check_launch("phase_from_phi_kernel");
@@ -369,7 +380,9 @@ extern "C" size_t nz_state_sort_static_capacity(void) { return kStaticSortScratc
 
 extern "C" int nz_state_sort_static(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out,
                                     void* stream) {
-  if (!in || !grid || coarsen <= 0) return set_error(NZ_ERR_ARG, "nz_state_sort_static: bad arguments");
+  int rc = check_grid(grid, "nz_state_sort_static");
+  if (rc) return rc;
+  if (!in || coarsen <= 0) return set_error(NZ_ERR_ARG, "nz_state_sort_static: bad arguments");
   const long long nbins = 1ll * ((grid->nx + coarsen - 1) / coarsen) * ((grid->ny + coarsen - 1) / coarsen) *
                           ((grid->nz + coarsen - 1) / coarsen);
   if (in->N < 0 || nbins > (1 << 26)) return set_error(NZ_ERR_ARG, "nz_state_sort_static: bad sizes");
@@ -380,7 +393,7 @@ extern "C" int nz_state_sort_static(const nz_state* in, const nz_grid* grid, int
                      "fixed %zu; use nz_state_sort with a caller buffer or coarsen the bins",
                      in->N, nbins, need, kStaticSortScratch);
   void* scratch = nullptr;
-  const int rc = static_sort_scratch(&scratch);
+  rc = static_sort_scratch(&scratch);
   if (rc != NZ_OK) return rc;
   return nz_state_sort(in, grid, coarsen, out, scratch, kStaticSortScratch, stream);
 }

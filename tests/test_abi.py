@@ -69,3 +69,130 @@ def test_scratch_sizes_and_more_argument_errors_without_gpu():
     # the moments walk with no substrate lists
     rc = lib.nz_walk_fused_moments(ctypes.byref(sub), None, 0, 0.005, None, None, 0, 10, None, None, 0, None, None)
     assert rc == _lib.NZ_ERR_ARG
+
+
+FAKE = 0x7F0000000000  # a 16-byte-aligned address the host never dereferences
+
+
+def _fused_substrate(_lib):
+    sub = _lib.Substrate()
+    sub.grid = _lib.Grid(8.0, 8.0, 8.0, 1.0, 1.0, 1.0, 8, 8, 8)
+    sub.nstructures, sub.S = 1, 4
+    for f in ("spheres", "cell_start", "cell_count", "cell_items", "cell_sph4", "cell_sid", "D", "T2"):
+        setattr(sub, f, FAKE)
+    return sub
+
+
+def _state(_lib, N, base=FAKE):
+    return _lib.State(N, base, base + 0x1000, base + 0x2000, base + 0x3000)
+
+
+def test_empty_inputs_return_ok_without_gpu():
+    """Zero walkers, zero items or an empty step range: every entry point
+    returns ok before any CUDA call, and null arrays are accepted where they
+    would hold nothing."""
+    import ctypes
+    from nozomi_b200 import _lib
+    lib = _lib.load()
+    by = ctypes.byref
+    sub = _fused_substrate(_lib)
+    draws = _lib.Draws(None, 0, 0, 1, 2, 0)
+    empty = _lib.State(0, None, None, None, None)
+    wk0 = _lib.Walkers()
+    wk0.N = 0
+    for mode in (0, _lib.MODE_SIG, _lib.MODE_PHI):
+        assert lib.nz_walk_step(by(sub), by(wk0), mode, 0.01, 0.0, 0.0, 0, by(draws), None) == 0
+    wk0.ndir = 3
+    assert lib.nz_walk_step(by(sub), by(wk0), _lib.MODE_PHASE, 0.01, 0.0, 0.0, 0, by(draws), None) == 0
+    assert lib.nz_state_pack(by(wk0), None, by(empty), None) == 0
+    assert lib.nz_state_unpack(by(empty), by(wk0), None) == 0
+    assert lib.nz_state_unpack_by_id(by(empty), by(wk0), None, None) == 0
+    assert lib.nz_walk_fused(by(sub), by(empty), _lib.MODE_PHI, 0.01, FAKE, FAKE, 0, 100, by(draws), None, None) == 0
+    # a non-empty state over an empty step range
+    st = _state(_lib, 1000)
+    assert lib.nz_walk_fused(by(sub), by(st), _lib.MODE_PHI, 0.01, FAKE, FAKE, 50, 50, by(draws), None, None) == 0
+    assert lib.nz_walk_fused_moments(by(sub), by(empty), 0, 0.01, None, None, 0, 100, by(draws), None, 0, FAKE,
+                                     None) == 0
+    assert lib.nz_walk_batch(FAKE, 3, FAKE, 0, _lib.MODE_PHI, 0, 100, FAKE, 148, 128, None) == 0
+    assert lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_PHI, 7, 7, FAKE, 148, 128, None) == 0
+    assert lib.nz_signal_phi(by(empty), FAKE, 6, FAKE, 4, FAKE, None) == 0
+    assert lib.nz_signal_phase(FAKE, 6, 0, FAKE, 4, FAKE, None) == 0
+    assert lib.nz_phase_from_phi(by(empty), FAKE, 6, None, None) == 0
+    assert lib.nz_moments(FAKE, FAKE, 0, FAKE, None) == 0
+    assert lib.nz_cells_gather(FAKE, 4, None, 0, None, None, 512, FAKE, None, None) == 0
+    grid = sub.grid
+    need = lib.nz_sort_scratch_bytes(0, 8 * 8 * 8)  # the histogram of the 8x8x8 grid's bins
+    assert need > 0
+    assert lib.nz_state_sort(by(empty), by(grid), 1, by(_lib.State(0, None, None, None, None)), FAKE, need, None) == 0
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    """Malformed calls that would otherwise launch a kernel on bad memory are
+    refused on the host with NZ_ERR_ARG (or NZ_ERR_CAPACITY) and a message."""
+    import ctypes
+    from nozomi_b200 import _lib
+    lib = _lib.load()
+    by = ctypes.byref
+    sub = _fused_substrate(_lib)
+    draws = _lib.Draws(None, 0, 0, 1, 2, 0)
+    N = 1000
+    a, b = _state(_lib, N), _state(_lib, N, FAKE + 0x100000)
+
+    def refused(rc, who, status=_lib.NZ_ERR_ARG):
+        assert rc == status, (who, rc)
+        assert who.encode() in lib.nz_last_error(), lib.nz_last_error()
+
+    grid = sub.grid
+    nb = 8 * 8 * 8
+    need = lib.nz_sort_scratch_bytes(N, nb)
+    assert lib.nz_state_sort_keyed(by(a), by(grid), 1, 0, by(b), FAKE, need - 4, None) == _lib.NZ_ERR_CAPACITY
+    bad_grid = _lib.Grid(8.0, 8.0, 8.0, 1.0, 1.0, 1.0, 8, 0, 8)
+    refused(lib.nz_state_sort(by(a), by(bad_grid), 1, by(b), FAKE, need, None), "nz_state_sort")
+    refused(lib.nz_state_sort_static(by(a), by(bad_grid), 1, by(b), None), "nz_state_sort_static")
+    refused(lib.nz_state_sort(by(a), by(grid), 1, by(a), FAKE, need, None), "nz_state_sort")  # in place
+    refused(lib.nz_state_sort(by(a), by(grid), 1, by(_state(_lib, N - 1, FAKE + 0x100000)), FAKE, need, None),
+            "nz_state_sort")
+    refused(lib.nz_state_sort(by(_state(_lib, N, FAKE + 8)), by(grid), 1, by(b), FAKE, need, None), "nz_state_sort")
+    refused(lib.nz_state_sort(by(_lib.State(N, FAKE, None, FAKE, FAKE)), by(grid), 1, by(b), FAKE, need, None),
+            "nz_state_sort")
+    refused(lib.nz_signal_phi(by(_lib.State(N, FAKE, FAKE, None, FAKE)), FAKE, 6, FAKE, 4, FAKE, None),
+            "nz_signal_phi")
+    refused(lib.nz_phase_from_phi(by(a), FAKE, 6, None, None), "nz_phase_from_phi")
+    refused(lib.nz_cells_gather(FAKE, 4, FAKE, 10, FAKE, FAKE, 0, FAKE, FAKE, None), "nz_cells_gather")
+    refused(lib.nz_cells_gather(FAKE, 4, FAKE, 10, FAKE, FAKE, 8, FAKE + 4, FAKE, None), "nz_cells_gather")
+    # fused walk: draw table, step range, moments limits, misaligned cell records
+    refused(lib.nz_walk_fused(by(sub), by(a), _lib.MODE_PHI, 0.01, FAKE, FAKE, 0, 10,
+                              by(_lib.Draws(FAKE, 10, 4, 1, 2, 0)), None, None), "nz_walk_fused")
+    refused(lib.nz_walk_fused(by(sub), by(a), _lib.MODE_PHI, 0.01, FAKE, FAKE, 10, 5, by(draws), None, None),
+            "nz_walk_fused")
+    refused(lib.nz_walk_fused(by(sub), by(a), _lib.MODE_MOMENTS, 0.01, None, None, 0, _lib.MOMENT_STEPS + 1,
+                              by(draws), FAKE, None), "nz_walk_fused")
+    refused(lib.nz_walk_fused(by(sub), by(a), _lib.MODE_PHI, 0.01, None, FAKE, 0, 10, by(draws), None, None),
+            "nz_walk_fused")
+    mis = _fused_substrate(_lib)
+    mis.cell_sph4 = FAKE + 4
+    refused(lib.nz_walk_fused(by(mis), by(a), 0, 0.01, None, None, 0, 10, by(draws), None, None), "nz_walk_fused")
+    near = _fused_substrate(_lib)
+    near.near_sph4, near.near_margin = FAKE, 0.5  # near records without their index arrays
+    refused(lib.nz_walk_fused(by(near), by(a), 0, 0.01, None, None, 0, 10, by(draws), None, None), "nz_walk_fused")
+    # moments walk: scratch below [steps][3][N] floats, or an unsupported mode
+    small = lib.nz_walk_fused_moments_scratch_bytes(N, 100) - 4
+    refused(lib.nz_walk_fused_moments(by(sub), by(a), 0, 0.01, None, None, 0, 100, by(draws), FAKE, small, FAKE,
+                                      None), "nz_walk_fused_moments")
+    refused(lib.nz_walk_fused_moments(by(sub), by(a), _lib.MODE_PHI, 0.01, FAKE, FAKE, 0, 100, by(draws), FAKE,
+                                      small + 4, FAKE, None), "nz_walk_fused_moments")
+    # batched walk: CTA shape, persistent grid without a queue, moments
+    refused(lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_PHI, 0, 100, FAKE, 148, 48, None), "nz_walk_batch")
+    refused(lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_PHI, 0, 100, FAKE, 148, 512, None), "nz_walk_batch")
+    refused(lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_PHI, 0, 100, None, 148, 128, None), "nz_walk_batch")
+    refused(lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_MOMENTS, 0, 100, FAKE, 148, 128, None), "nz_walk_batch")
+    # plain step: unknown mode bits, phase without directions, null positions
+    wk = _lib.Walkers()
+    wk.N, wk.spins, wk.spins0 = N, FAKE, FAKE
+    refused(lib.nz_walk_step(by(sub), by(wk), 64, 0.01, 0.0, 0.0, 0, by(draws), None), "nz_walk_step")
+    refused(lib.nz_walk_step(by(sub), by(wk), _lib.MODE_PHASE, 0.01, 0.0, 0.0, 0, by(draws), None), "nz_walk_step")
+    wk.spins = None
+    refused(lib.nz_walk_step(by(sub), by(wk), 0, 0.01, 0.0, 0.0, 0, by(draws), None), "nz_walk_step")
+    # packing: walker count mismatch
+    wk.spins, wk.N = FAKE, N + 1
+    refused(lib.nz_state_pack(by(wk), None, by(a), None), "nz_state_pack")
