@@ -50,6 +50,8 @@ def lib():
         _lib.oz_segments.restype = ctypes.c_int
         _lib.oz_seed_accept.argtypes = [_P, _P, i, _P, _P]
         _lib.oz_philox_normals.argtypes = [u, u, u, i, i, i, _P]
+        _lib.oz_philox_block.argtypes = [_P, u, u]
+        _lib.oz_box_muller_pairs.argtypes = [_P, _P, i, _P]
         _lib.oz_moments.argtypes = [i, _P, _P, _P]
         _lib.oz_signal_phi.argtypes = [i, _P, _P, i, _P, i, _P, _P]
         _lib.oz_signal_phase.argtypes = [i, _P, i, _P, i, _P, _P]
@@ -59,7 +61,8 @@ def lib():
         _lib.oz_set_phase64.restype = None
         for fn in ("oz_walk_f32", "oz_walk_f64", "oz_seed", "oz_seed_range"):
             getattr(_lib, fn).restype = ctypes.c_int
-        for fn in ("oz_seed_accept", "oz_philox_normals", "oz_moments", "oz_signal_phi", "oz_signal_phase"):
+        for fn in ("oz_seed_accept", "oz_philox_normals", "oz_philox_block", "oz_box_muller_pairs", "oz_moments",
+                   "oz_signal_phi", "oz_signal_phase"):
             getattr(_lib, fn).restype = None
     return _lib
 
@@ -222,7 +225,26 @@ def seed_accept(geom: Geometry, targets, pos):
     return out.astype(bool)
 
 
+def philox_block(counter, key0: int, key1: int) -> np.ndarray:
+    """One Philox4x32-10 block of the 4-word counter under key (key0, key1)."""
+    c = np.ascontiguousarray(np.asarray(counter, dtype=np.uint64) & 0xFFFFFFFF, dtype=np.uint32).copy()
+    lib().oz_philox_block(c.ctypes.data, key0 & 0xFFFFFFFF, key1 & 0xFFFFFFFF)
+    return c
+
+
+def box_muller_pairs(ua, ub) -> np.ndarray:
+    """The oracle's Box-Muller transform of 32-bit word pairs: [n, 2] float32."""
+    ua = np.ascontiguousarray(ua, np.uint32)
+    ub = np.ascontiguousarray(ub, np.uint32)
+    out = np.zeros((ua.size, 2), np.float32)
+    lib().oz_box_muller_pairs(ua.ctypes.data, ub.ctypes.data, ua.size, out.ctypes.data)
+    return out
+
+
 def philox_normals(key0: int, key1: int, stream: int, N: int, step: int, ndraw: int):
+    """Normals [N, ndraw, 3] of draws 0..ndraw-1 of walkers 0..N-1 at `step`:
+    counter (walker, step, draw, stream); words 0, 1 and 2, 3 go through one
+    Box-Muller each, the last normal of the second pair unused."""
     out = np.zeros((N, ndraw, 3), np.float32)
     lib().oz_philox_normals(key0 & 0xFFFFFFFF, key1 & 0xFFFFFFFF, stream, N, step, ndraw, out.ctypes.data)
     return out

@@ -295,6 +295,14 @@ OZ_API void oz_seed_accept(const oz_geom* g, const unsigned char* target, int N,
     }
 }
 
+/* One Philox4x32-10 block, in place: c[4] counter, (k0, k1) key. */
+OZ_API void oz_philox_block(uint32_t* c, uint32_t k0, uint32_t k1) { oz_philox4x32_10(c, k0, k1); }
+
+/* The Box-Muller pair of n word pairs: out[2i], out[2i+1] from (ua[i], ub[i]). */
+OZ_API void oz_box_muller_pairs(const uint32_t* ua, const uint32_t* ub, int n, float* out) {
+    for (int i = 0; i < n; ++i) oz_box_muller(ua[i], ub[i], out + 2 * i, out + 2 * i + 1);
+}
+
 /* Normals of draws [0, ndraw) of every walker at one step: out[w][d][3]. */
 OZ_API void oz_philox_normals(uint32_t key0, uint32_t key1, uint32_t stream, int N, int step, int ndraw,
                               float* out) {
