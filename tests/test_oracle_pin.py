@@ -109,3 +109,42 @@ def test_seeding_rule_matches_seedSpinsKernel():
         acc = oz.seed_accept(g, z[f"{t}_targets"], pos)
         np.testing.assert_array_equal(acc, z[f"{t}_accept"])
         np.testing.assert_array_equal(pos[:, acc], z[f"{t}_pos"][:, acc])
+
+
+def test_oracle_equals_reference_kernel_on_packed_substrate():
+    """The headline substrate (200 packed beaded axons, 29,628 spheres with
+    images, 40x40x80 um, 1 um cells, the reference's padded table K = 45):
+    the reference's own randomWalk3d_phase_multidirr (sim3d_kernel.cu:719-943,
+    compiled for the CPU with the template DiffSim3d fills in) and the oracle
+    walk 16,000 seeded walkers through the first 400 waveform samples (the
+    first gradient lobe, 30 directions) with the same Philox draws: positions,
+    spins0 and phase bit for bit."""
+    import sys
+    from pathlib import Path
+    from oracle.build import reference_named
+    from oracle.cells_oracle import padded_as_lists
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    import bench
+    if reference_named(bench.REF_CPU_BUILD) is None:
+        pytest.skip("oracle/_ref reference build absent (the reference tree was absent at build)")
+    sub, pg, dirs, _ = bench.workload()
+    ref = bench.ReferenceCpu(sub, pg, dirs)
+    N, K, nsteps = ref.N, ref.K, 400
+    x0 = ref.spins.reshape(3, N).copy()
+    ref.run(nsteps)
+    _, pars = reference_named(bench.REF_CPU_BUILD)
+    nseg = (int(pars["nLx"]), int(pars["nLy"]), int(pars["nLz"]))
+    st, ct, it = padded_as_lists(K, ref.seg, nseg[0] * nseg[1] * nseg[2])
+    ns = sub.nstructures
+    g = oz.Geometry(sub.spheres().astype(np.float32), ns, sub.L, nseg, st, ct, it,
+                    np.full(ns + 1, 2.0, np.float32), np.full(ns + 1, 100.0, np.float32),
+                    dL=(float(pars["dLx"]), float(pars["dLy"]), float(pars["dLz"])))
+    spins, spins0 = x0.copy(), x0.copy()
+    phase = np.zeros((dirs.shape[1], N), np.float32)
+    oz.walk_f32(g, oz.philox(1000), oz.MODE_PHASE, spins, spins0, 0, nsteps, float(pg.dt), G=ref.G, Garea=ref.Ga,
+                phase=phase, diffdir=dirs.astype(np.float32))
+    np.testing.assert_array_equal(spins, ref.spins.reshape(3, N))
+    np.testing.assert_array_equal(spins0, ref.spins0.reshape(3, N))
+    np.testing.assert_array_equal(phase, ref.phase.reshape(-1, N))
+    # and not trivially: the walkers moved and accrued phase
+    assert np.abs(spins - x0).max() > 0.5 and np.abs(phase).max() > 0
