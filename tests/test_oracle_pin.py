@@ -111,14 +111,9 @@ def test_seeding_rule_matches_seedSpinsKernel():
         np.testing.assert_array_equal(pos[:, acc], z[f"{t}_pos"][:, acc])
 
 
-def test_oracle_equals_reference_kernel_on_packed_substrate():
-    """The headline substrate (200 packed beaded axons, 29,628 spheres with
-    images, 40x40x80 um, 1 um cells, the reference's padded table K = 45):
-    the reference's own randomWalk3d_phase_multidirr (sim3d_kernel.cu:719-943,
-    compiled for the CPU with the template DiffSim3d fills in) and the oracle
-    walk 16,000 seeded walkers through the first 400 waveform samples (the
-    first gradient lobe, 30 directions) with the same Philox draws: positions,
-    spins0 and phase bit for bit."""
+def _packed_reference():
+    """The reference kernel's CPU build for the packed substrate, its oracle
+    geometry over the same padded table, and the seeded start positions."""
     import sys
     from pathlib import Path
     from oracle.build import reference_named
@@ -129,16 +124,27 @@ def test_oracle_equals_reference_kernel_on_packed_substrate():
         pytest.skip("oracle/_ref reference build absent (the reference tree was absent at build)")
     sub, pg, dirs, _ = bench.workload()
     ref = bench.ReferenceCpu(sub, pg, dirs)
-    N, K, nsteps = ref.N, ref.K, 400
-    x0 = ref.spins.reshape(3, N).copy()
-    ref.run(nsteps)
     _, pars = reference_named(bench.REF_CPU_BUILD)
     nseg = (int(pars["nLx"]), int(pars["nLy"]), int(pars["nLz"]))
-    st, ct, it = padded_as_lists(K, ref.seg, nseg[0] * nseg[1] * nseg[2])
+    st, ct, it = padded_as_lists(ref.K, ref.seg, nseg[0] * nseg[1] * nseg[2])
     ns = sub.nstructures
     g = oz.Geometry(sub.spheres().astype(np.float32), ns, sub.L, nseg, st, ct, it,
                     np.full(ns + 1, 2.0, np.float32), np.full(ns + 1, 100.0, np.float32),
                     dL=(float(pars["dLx"]), float(pars["dLy"]), float(pars["dLz"])))
+    return ref, g, pg, dirs, ref.spins.reshape(3, ref.N).copy()
+
+
+def test_oracle_equals_reference_kernel_on_packed_substrate():
+    """The headline substrate (200 packed beaded axons, 29,628 spheres with
+    images, 40x40x80 um, 1 um cells, the reference's padded table K = 45):
+    the reference's own randomWalk3d_phase_multidirr (sim3d_kernel.cu:719-943,
+    compiled for the CPU with the template DiffSim3d fills in) and the oracle
+    walk 16,000 seeded walkers through the first 400 waveform samples (the
+    first gradient lobe, 30 directions) with the same Philox draws: positions,
+    spins0 and phase bit for bit."""
+    ref, g, pg, dirs, x0 = _packed_reference()
+    N, nsteps = ref.N, 400
+    ref.run(nsteps)
     spins, spins0 = x0.copy(), x0.copy()
     phase = np.zeros((dirs.shape[1], N), np.float32)
     oz.walk_f32(g, oz.philox(1000), oz.MODE_PHASE, spins, spins0, 0, nsteps, float(pg.dt), G=ref.G, Garea=ref.Ga,
@@ -148,3 +154,45 @@ def test_oracle_equals_reference_kernel_on_packed_substrate():
     np.testing.assert_array_equal(phase, ref.phase.reshape(-1, N))
     # and not trivially: the walkers moved and accrued phase
     assert np.abs(spins - x0).max() > 0.5 and np.abs(phase).max() > 0
+
+
+@pytest.mark.parametrize("kernel", ["randomWalk3d", "randomWalk3d_phase"])
+def test_oracle_equals_reference_narrow_and_three_axis_kernels_on_packed_substrate(kernel):
+    """The reference's other two walks on the same substrate and build, 300
+    steps of 16,000 walkers with the same Philox draws: randomWalk3d
+    (sim3d_kernel.cu:340-522, T2 weighting) against the oracle's SIG mode
+    (positions bit for bit, sig to expf ulps), and randomWalk3d_phase
+    (:524-717, fixed x, y, z) against the oracle's PHASE mode with the
+    identity as directions (bit for bit)."""
+    import ctypes
+    ref, g, pg, _, x0 = _packed_reference()
+    N, nsteps, dt = ref.N, 300, float(pg.dt)
+    P, f, i = ctypes.c_void_p, ctypes.c_float, ctypes.c_int
+    lib = ref.lib
+    spins = x0.reshape(-1).copy()  # the reference walks these in place; x0 stays the start
+    spins0 = spins.copy()
+    if kernel == "randomWalk3d":
+        lib.ref_run_walk.argtypes = [i, i, i, f, P, P, P, P, P]
+        sig_ref = np.ones(N, np.float32)
+        for n in range(nsteps):
+            lib.ref_run_walk(N // 1000, 1000, n, dt, ref.sph.ctypes.data, ref.seg.ctypes.data, spins.ctypes.data,
+                             spins0.ctypes.data, sig_ref.ctypes.data)
+        x, x00, sig = x0.copy(), x0.copy(), np.ones(N, np.float32)
+        oz.walk_f32(g, oz.philox(1000), oz.MODE_SIG, x, x00, 0, nsteps, dt, sig=sig)
+        np.testing.assert_allclose(sig, sig_ref, rtol=2e-6)
+        assert sig.min() < 1.0
+    else:
+        lib.ref_run_walk_phase.argtypes = [i, i, i, f, P, P, P, P, P, f, f]
+        ph_ref = np.zeros(3 * N, np.float32)
+        for n in range(nsteps):
+            lib.ref_run_walk_phase(N // 1000, 1000, n, dt, ref.sph.ctypes.data, ref.seg.ctypes.data,
+                                   spins.ctypes.data, spins0.ctypes.data, ph_ref.ctypes.data, f(ref.G[n]),
+                                   f(ref.Ga[n]))
+        x, x00, ph = x0.copy(), x0.copy(), np.zeros((3, N), np.float32)
+        oz.walk_f32(g, oz.philox(1000), oz.MODE_PHASE, x, x00, 0, nsteps, dt, G=ref.G, Garea=ref.Ga, phase=ph,
+                    diffdir=np.eye(3, dtype=np.float32))
+        np.testing.assert_array_equal(ph, ph_ref.reshape(3, N))
+        assert np.abs(ph).max() > 0
+    np.testing.assert_array_equal(x, spins.reshape(3, N))
+    np.testing.assert_array_equal(x00, spins0.reshape(3, N))
+    assert np.abs(x - x0).max() > 0.5
