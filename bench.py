@@ -366,9 +366,6 @@ def run_ours(args):
         run.walk(walk_events)
         return run.signal_sums()
 
-    n_chunks = -(-run.nsteps // tuning.steps_per_launch)
-    # kernels per step: pack, then per chunk (memset-free) bin_count + scan + scatter + walk, then signal
-    launches_per_step = 1 + 4 * n_chunks + 1
 
     # FP32 peak of this GPU (probe kernel), before the timed region
     sms = torch.cuda.get_device_properties(local).multi_processor_count
@@ -424,6 +421,10 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     eager_ms = e0.elapsed_time(e1)
+    # library kernels of one step (pack; per chunk the re-binning's bin count,
+    # histogram scan and scatter, and the fused walk; the signal), as counted
+    # by the run while it launched them
+    launches_per_step = run.launches
     walk_ms = sum(a.elapsed_time(b) for a, b in ev)
     n_walk = len(ev)
 

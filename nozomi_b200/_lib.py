@@ -15,6 +15,7 @@ MODE_SIG, MODE_PHASE, MODE_PHI, MODE_MOMENTS, MODE_TANGENT64 = 1, 2, 4, 8, 16
 FLAG_DRAWS_EXHAUSTED, FLAG_ITER_CAP, FLAG_UNSEEDED = 1, 2, 4
 FUSED_THREADS = 128       # walkers per CTA / per work item of the fused and batched walks
 MOMENT_STEPS = 256        # steps per launch when the fused walk accumulates moments
+SCAN_SINGLE_KEYS = 32768  # nz_state_sort scans up to this many bins in one kernel, beyond it in three
 
 _P = ctypes.c_void_p
 _i = ctypes.c_int

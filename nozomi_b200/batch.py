@@ -215,9 +215,18 @@ class BatchRun:
         return self.prepare().run()
 
     def launches(self) -> int:
-        """Kernels per run: per chunk 3 per active job (re-bin) + 1 batch walk;
-        one signal per job."""
-        return sum(3 * len(c["active"]) + 1 for c in self.chunks) + len(self.jobs)
+        """Library kernels of one step (prepare + run): a pack per job; per
+        chunk each active job's re-binning (FusedState.sort_kernels) and one
+        batched walk; a signal per job."""
+        nl_on = self.tuning.by_label
+        n = sum(1 for j in self.jobs if j["N"]) * 2  # pack and signal
+        for c in self.chunks:
+            for i in c["active"]:
+                j = self.jobs[i]
+                n += j["buf"][0].sort_kernels(j["sub"].grid, self.tuning.coarsen,
+                                              j["sub"].nstructures + 1 if nl_on else 0)
+            n += 1 if c["items"].shape[0] else 0
+        return n
 
     def signals(self) -> list:
         res = []

@@ -105,7 +105,7 @@ __global__ void scan_kernel(const int* __restrict__ in, int* __restrict__ out, i
 // beyond that (with tile_sums and tile_offsets of scan_tiles(n) ints each)
 // one CTA per kScanTile ints.
 constexpr int kScanTile = 8192;
-constexpr int kScanSingle = 32768;
+constexpr int kScanSingle = 32768;  // mirrored as SCAN_SINGLE_KEYS in nozomi_b200/_lib.py (launch counts)
 int scan_tiles(int n);
 int exclusive_scan(const int* in, int* out, int n, int* tile_sums, int* tile_offsets, cudaStream_t st);
 

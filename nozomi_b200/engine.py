@@ -325,11 +325,23 @@ class FusedState:
     def walker_ids(self) -> torch.Tensor:
         return self.org[:, 3].contiguous().view(torch.int32)
 
+    @staticmethod
+    def sort_bins(grid: L.Grid, coarsen: int, nlabels: int = 0) -> int:
+        """Keys of a re-binning: coarsened cells, times labels when nlabels > 0."""
+        return (-(-grid.nx // coarsen)) * (-(-grid.ny // coarsen)) * (-(-grid.nz // coarsen)) * max(nlabels, 1)
+
+    def sort_kernels(self, grid: L.Grid, coarsen: int, nlabels: int = 0) -> int:
+        """Library kernels one sort_into launches: bin count, the histogram
+        scan (one kernel, or three above SCAN_SINGLE_KEYS bins), scatter."""
+        if self.N == 0:
+            return 0
+        return 2 + (1 if self.sort_bins(grid, coarsen, nlabels) <= L.SCAN_SINGLE_KEYS else 3)
+
     def sort_into(self, other: "FusedState", grid: L.Grid, coarsen: int, scratch: torch.Tensor | None = None,
                   nlabels: int = 0):
         """Re-bin into `other` by cell (coarsened), or by (label, cell) when
         nlabels > 0.  Returns the scratch buffer for reuse."""
-        nb = (-(-grid.nx // coarsen)) * (-(-grid.ny // coarsen)) * (-(-grid.nz // coarsen)) * max(nlabels, 1)
+        nb = self.sort_bins(grid, coarsen, nlabels)
         need = int(L.load().nz_sort_scratch_bytes(self.N, nb))
         if scratch is None or scratch.numel() < need:
             scratch = torch.empty(need, dtype=torch.uint8, device=_dev())

@@ -89,7 +89,7 @@ class DwiRun:
             ids = torch.arange(self.id0, self.id0 + N, dtype=torch.int64, device=x.device).to(torch.int32)
         self.state = engine.FusedState.from_walkers(wk, ids)
         self.spare = engine.FusedState(N)
-        self.launches = 1
+        self.launches = 1 if N else 0  # library kernels since prepare: the pack
         return self
 
     def walk(self, events: list | None = None):
@@ -100,6 +100,7 @@ class DwiRun:
         nl = self.sub.nstructures + 1 if t.by_label else 0
         stream = torch.cuda.current_stream()
         for s0 in range(0, self.nsteps, t.steps_per_launch):
+            self.launches += self.state.sort_kernels(self.sub.grid, t.coarsen, nl) + (1 if self.state.N else 0)
             self._scratch = self.state.sort_into(self.spare, self.sub.grid, t.coarsen, self._scratch, nlabels=nl)
             self.state, self.spare = self.spare, self.state
             if events is not None:
@@ -110,13 +111,12 @@ class DwiRun:
             if events is not None:
                 e1.record(stream)
                 events.append((e0, e1))
-            self.launches += 4
         return self
 
     def signal_sums(self) -> torch.Tensor:
         """[2, ndir, nb] float64 sums over walkers of cos / sin."""
         out = self.state.signal(self.dirs, self.amps)
-        self.launches += 1
+        self.launches += 1 if self.state.N else 0
         return out
 
     def signal(self) -> np.ndarray:

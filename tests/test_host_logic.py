@@ -69,3 +69,27 @@ def test_autotune_signature():
     b = _small_specs()
     b[0] = __import__("dataclasses").replace(b[0], N=b[0].N * 50)
     assert signature(b) != signature(a)
+
+
+def test_rebinning_kernel_count_follows_the_scan_threshold():
+    """The launch counts bench.py reports: a re-binning launches bin count,
+    scan and scatter, the scan as three kernels above SCAN_SINGLE_KEYS bins
+    (the mirror of kScanSingle in csrc/kernels.cuh), none for no walkers."""
+    import re
+    from pathlib import Path
+    from nozomi_b200 import _lib as L
+    from nozomi_b200.engine import FusedState, box_grid
+    src = (Path(__file__).resolve().parents[1] / "nozomi_b200" / "csrc" / "kernels.cuh").read_text()
+    assert int(re.search(r"kScanSingle = (\d+);", src).group(1)) == L.SCAN_SINGLE_KEYS
+    st = object.__new__(FusedState)  # only N is read: no device buffers needed
+    st.N = 1000
+    packed = box_grid((40.0, 40.0, 80.0), (80, 80, 160))  # 0.5 um cells of the packed box
+    assert FusedState.sort_bins(packed, 8) == 10 * 10 * 20
+    assert st.sort_kernels(packed, 8) == 3
+    assert FusedState.sort_bins(packed, 8, nlabels=201) == 402_000
+    assert st.sort_kernels(packed, 8, nlabels=201) == 5
+    edge = box_grid((32.0, 32.0, 32.0), (32, 32, 32))
+    assert FusedState.sort_bins(edge, 1) == L.SCAN_SINGLE_KEYS and st.sort_kernels(edge, 1) == 3
+    assert st.sort_kernels(edge, 1, nlabels=2) == 5
+    st.N = 0
+    assert st.sort_kernels(packed, 8, nlabels=201) == 0
