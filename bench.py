@@ -206,7 +206,8 @@ class ReferenceCpu:
 
 def reference_cpu_sample(sub, pg, dirs, seconds, steps=1, warmup=0):
     """Time the reference kernel's CPU build: `warmup` + `steps` samples of
-    about `seconds` each.  Returns (walker-steps/s, cores, sample text)."""
+    about `seconds` each.  Returns (walker-steps/s, cores, sample text, ms per
+    timed sample)."""
     cores = os.cpu_count() or 1
     r = ReferenceCpu(sub, pg, dirs)
     t = time.perf_counter()
@@ -219,7 +220,7 @@ def reference_cpu_sample(sub, pg, dirs, seconds, steps=1, warmup=0):
     el = time.perf_counter() - t
     sample = (f"{r.N} walkers x {per} launches per step x {steps} step(s) (waveform samples "
               f"{5 + per * warmup}..{5 + per * (warmup + steps) - 1}), {el:.1f} s, padded K={r.K}")
-    return r.N * per * steps / el, cores, sample
+    return r.N * per * steps / el, cores, sample, el * 1e3 / steps
 
 
 def run_reference(args):
@@ -230,8 +231,8 @@ def run_reference(args):
     from oracle.build import build_oracle
     build_oracle()
     try:
-        value, cores, sample = reference_cpu_sample(sub, pg, dirs, args.cpu_seconds / 2, steps=args.steps,
-                                                    warmup=args.warmup)
+        value, cores, sample, ms_step = reference_cpu_sample(sub, pg, dirs, args.cpu_seconds / 2, steps=args.steps,
+                                                             warmup=args.warmup)
         kind, how = "reference", REF_CPU_KIND
     except (FileNotFoundError, ValueError) as e:  # no reference build on this host: the C restatement
         total_t, total_ws = 0.0, 0
@@ -242,10 +243,11 @@ def run_reference(args):
                 total_ws += 1
                 total_t += 1.0 / v
         value = total_ws / total_t
+        ms_step = None  # samples of differing walker counts: no common step time
         kind, how = "port", f"oracle/walk_oracle.c, the C restatement of the kernel, OpenMP over walkers ({e})"
     line = {"impl": "reference", "metric": "walker-steps/s", "value": value, "unit": "walker-steps/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "cell_um": 1.0},
             "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": kind,
                              "sample": sample + "; " + how},
@@ -474,7 +476,7 @@ def run_ours(args):
             port = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "port",
                     "sample": sample + "; oracle/walk_oracle.c, OpenMP over walkers"}
             try:
-                v, cores, sample = reference_cpu_sample(sub, pg, dirs, args.cpu_seconds / 2)
+                v, cores, sample, _ = reference_cpu_sample(sub, pg, dirs, args.cpu_seconds / 2)
                 cpu = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "reference",
                        "sample": sample + "; " + REF_CPU_KIND, "port": port}
             except (FileNotFoundError, ValueError) as e:

@@ -41,3 +41,33 @@ def test_reference_cpu_arm_runs_a_short_sample():
     assert np.isfinite(x).all() and not np.array_equal(r.spins, x0)
     L = np.array(sub.L)[:, None]
     assert np.all(np.abs(x) <= L / 2 + 1e-4)
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` runs on the host cores alone (no GPU) and
+    prints one JSON line with the base contract's keys, its cpu_baseline and
+    an e2e without transfers; the same metric, unit and workload as the GPU
+    arm."""
+    import json
+    import subprocess
+    import bench
+    from oracle.build import reference_named
+    if reference_named(bench.REF_CPU_BUILD) is None:
+        pytest.skip("oracle/_ref reference build absent (the reference tree was absent at build)")
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "2",
+                          "--warmup", "1", "--cpu-seconds", "1"], cwd=ROOT, capture_output=True, text=True,
+                         timeout=600, check=True).stdout
+    lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["metric"] == "walker-steps/s" and d["unit"] == "walker-steps/s"
+    assert d["higher_is_better"] is True and d["steps"] == 2 and d["warmup"] == 1
+    assert d["config"]["workload"] == bench.WORKLOAD
+    assert d["value"] > 0 and d["ms_per_step"] > 0
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "walker-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
