@@ -9,6 +9,8 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 
 NARROW = ["narrow_sphere_in", "narrow_sphere_out", "narrow_chain_in", "narrow_chain_out", "narrow_periodic_in"]
 DWI = ["dwi_c1", "dwi_c1_cells", "dwi_overlap", "dwi_overlap_3axis"]
+# walkers started on box faces, edges, corners and cell boundaries (the oracle's pin)
+EDGE = ["dwi_faces"]
 
 
 def load(name: str) -> dict:

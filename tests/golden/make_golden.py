@@ -3,9 +3,10 @@
 Run in a container that holds the reference tree (default /root/reference,
 override with NOZOMI_REFERENCE_ROOT):
 
-    python tests/golden/make_golden.py [ingestion]
+    python tests/golden/make_golden.py [ingestion | faces]
 
-(``ingestion`` regenerates only tests/golden/ingestion.npz.)  The reference's own Python engine (DiffSim3d / DwiSim3d / SimGeometry3D,
+(``ingestion`` regenerates only tests/golden/ingestion.npz, ``faces`` only
+tests/golden/dwi_faces.npz.)  The reference's own Python engine (DiffSim3d / DwiSim3d / SimGeometry3D,
 simulation_toolkit/simulation_engine/) is imported with a host stand-in for
 pycuda (oracle/fake_pycuda.py); its ``SourceModule`` compiles the reference's
 own template-substituted kernel source (sim3d_kernel.cu) for the CPU.  Draws are
@@ -266,12 +267,57 @@ def ingestion_case(ag, tmpdir):
                         fibres=np.concatenate(out))
 
 
+def faces_case(ds3, geo, wf):
+    """Walkers started on the box and cell boundaries: a non-cubic 6 x 5 x 7 um
+    box with 4 x 3 x 5 cells (edges 1.5, 5/3 and 1.4 um, none a power of two),
+    spheres of two structures crossing every face, 10 directions.  Of 1000
+    walkers, 400 start on a face, an edge or a corner of the box, exactly or
+    one float32 ulp inside or outside, and 200 exactly on interior cell
+    boundaries (x = -L/2 + k dL in float32); the rest uniformly in the box."""
+    rng = np.random.default_rng(11)
+    L = np.array([6.0, 5.0, 7.0])
+    structs = []
+    for k, Dk in enumerate((1.2, 0.8)):
+        m = 10
+        c = rng.uniform(-0.5, 0.5, (3, m)) * L[:, None]
+        for i in range(6):  # one sphere centred on each face
+            c[i // 2, i] = (1 if i % 2 else -1) * L[i // 2] / 2
+        structs.append((c[0], c[1], c[2], rng.uniform(0.5, 1.3, m), Dk))
+    N = 1000
+    x0 = (rng.uniform(-0.5, 0.5, (3, N)) * L[:, None]).astype(np.float32)
+    half = (L / 2).astype(np.float32)
+    for w in range(400):
+        nax = 1 + w % 3  # a face, an edge or a corner
+        axes = rng.choice(3, nax, replace=False)
+        for a in axes:
+            v = half[a] if rng.random() < 0.5 else -half[a]
+            step = (w // 3) % 3  # exactly, one ulp toward +inf, one toward -inf
+            if step == 1:
+                v = np.nextafter(v, np.float32(np.inf))
+            elif step == 2:
+                v = np.nextafter(v, np.float32(-np.inf))
+            x0[a, w] = v
+    nseg = (4, 3, 5)
+    dL = (L / np.array(nseg)).astype(np.float32)
+    for w in range(400, 600):
+        a = w % 3
+        k = rng.integers(1, nseg[a])
+        x0[a, w] = np.float32(-half[a] + np.float32(k) * dL[a])
+    dirs = rng.standard_normal((3, 10))
+    dirs /= np.linalg.norm(dirs, axis=0)
+    pg = wf.PGDiffWaveform(2.0, 1.0, 3.0, time_step=0.01)
+    dwi_case(ds3, geo, wf, "dwi_faces", tuple(L), structs, None, nseg, N, pg, dirs, 2.0, 505, custom_x0=x0)
+
+
 def main():
     ds3, geo, wf, ag = _load_reference()
     if sys.argv[1:] == ["ingestion"]:
         import tempfile
         with tempfile.TemporaryDirectory() as d:
             ingestion_case(ag, d)
+        return
+    if sys.argv[1:] == ["faces"]:
+        faces_case(ds3, geo, wf)
         return
     import tempfile
     with tempfile.TemporaryDirectory() as d:
@@ -331,6 +377,7 @@ def main():
              custom_x0=x0)
     dwi_case(ds3, geo, wf, "dwi_overlap_3axis", (6.0, 6.0, 6.0), structs, None, (1, 1, 1), N, pg_short,
              np.eye(3), 2.5, 304, custom_x0=x0, three_axis=True)
+    faces_case(ds3, geo, wf)
 
 
 if __name__ == "__main__":

@@ -9,7 +9,7 @@ the positions seedSpinsKernel accepts.
 import numpy as np
 import pytest
 
-from tests._fixtures import DWI, NARROW, dirs_of, load, oracle_geometry
+from tests._fixtures import DWI, EDGE, NARROW, dirs_of, load, oracle_geometry
 from oracle import oracle as oz
 from oracle.cells_oracle import cells_members, segments_reference
 
@@ -30,7 +30,7 @@ def test_narrow_pulse_bit_exact(name):
     assert (r["flags"] & oz.FLAG_DRAWS_EXHAUSTED).sum() == 0
 
 
-@pytest.mark.parametrize("name", DWI)
+@pytest.mark.parametrize("name", DWI + EDGE)
 def test_dwi_phase_bit_exact(name):
     c = load(name)
     g = oracle_geometry(c)
@@ -59,7 +59,7 @@ def test_segments_match_set_segments():
         K, seg = segments_reference(z[f"case{i}_spheres"], tuple(z[f"case{i}_L"]), tuple(z[f"case{i}_nseg"]))
         assert K == int(z[f"case{i}_K"])
         np.testing.assert_array_equal(seg, z[f"case{i}_segments"])
-    for name in NARROW + DWI:
+    for name in NARROW + DWI + EDGE:
         c = load(name)
         nseg = tuple(int(v) for v in c["nseg"])
         K, seg = segments_reference(c["spheres"], tuple(c["L"]), nseg)
