@@ -1,4 +1,4 @@
-"""The reference's own walk kernel on the GPU: a BASELINE, not the product.
+"""The reference's own walk kernel on the GPU: a baseline, not the product.
 
 nozomi runs its walk as CUDA through pycuda: DiffSim3d fills the %-template
 of simulation_toolkit/simulation_engine/sim3d_kernel.cu with the run's
