@@ -7,11 +7,12 @@ compartment, then walks all steps in fused launches that accumulate the
 per-step displacement moments on the device (the reference launches a walk
 and a moment kernel per step).  Writes
 ``<substrate dir>/../sim/ADCdata/diffcoeff_<compartment>_<nseg>segments_<N>spins_<name>_TABLEtime<s>sec_SIMtime<s>sec_timestep<dt>ms.pkl``
-holding ``np.column_stack((Dx, Dy, Dz, t))`` as the reference does, and the
-kurtoses beside it.
+holding ``np.column_stack((Dx, Dy, Dz, t))`` as the reference does, the
+kurtoses beside it, and a JSON record of the run's timings and sizes.
 """
 from __future__ import annotations
 
+import json
 import os
 import pickle
 import time
@@ -48,6 +49,18 @@ def narrow_pulse(sim: DiffSim3d, nt: int, dt: float):
     return t, Dv, K
 
 
+def write_run_record(path, **fields):
+    """The run's metrics as JSON beside its pickles (the reference keeps its
+    timings only in the output file name): table and walk seconds, walkers,
+    steps, and walker-steps/s of the walk."""
+    rec = dict(fields)
+    walk_s = float(rec.get("sim_time_s") or 0.0)
+    rec["walker_steps_per_s"] = (rec["num_spins"] * rec["steps"] / walk_s) if walk_s > 0 else None
+    with open(path, "w") as f:
+        json.dump(rec, f, indent=1)
+    return rec
+
+
 def simulation_main(params, substrate_file):
     sim_time = float(params['sim_time'])
     dt = float(params['time_step'])
@@ -71,7 +84,8 @@ def simulation_main(params, substrate_file):
     t1 = time.time()
     t, Dv, K = narrow_pulse(sim, nt, dt)
     torch.cuda.synchronize()
-    sim_elapsed = round(time.time() - t1, 2)
+    walk_s = time.time() - t1
+    sim_elapsed = round(walk_s, 2)
     base = os.path.splitext(os.path.basename(substrate_file))[0]
     name = (f"diffcoeff_{compartment}_{nseg}segments_{N}spins_{base}_TABLEtime{table_time}sec_"
             f"SIMtime{sim_elapsed}sec_timestep{dt}ms")
@@ -82,5 +96,9 @@ def simulation_main(params, substrate_file):
         pickle.dump(np.column_stack((Dv[:, 0], Dv[:, 1], Dv[:, 2], t)), f)
     with open(os.path.join(out_dir, name + '_kurtosis.pkl'), 'wb') as f:
         pickle.dump(np.column_stack((K[:, 0], K[:, 1], K[:, 2], t)), f)
+    write_run_record(os.path.join(out_dir, name + '.json'), substrate=os.path.abspath(substrate_file),
+                     compartment=compartment, num_spins=N, steps=nt, time_step_ms=dt, nseg=nseg,
+                     table_time_s=float(table_time), sim_time_s=float(walk_s), D_final=Dv[-1].tolist(),
+                     K_final=K[-1].tolist())
     print(f"simulation completed: {path}")
     return path

@@ -57,6 +57,8 @@ def test_cli_end_to_end(tmp_path):
     out = list((root / "run1" / "sim" / "ADCdata").glob("diffcoeff_intra_*spins_sub_*.pkl"))
     data = pickle.load(open([p for p in out if "kurtosis" not in p.name][0], "rb"))
     assert data.shape == (500, 4)
+    rec = json.loads(next((root / "run1" / "sim" / "ADCdata").glob("*.json")).read_text())
+    assert rec["num_spins"] == 20000 and rec["steps"] == 500 and rec["walker_steps_per_s"] > 0
     # fibres along z: free along z, restricted across
     assert 1.6 < data[-1, 2] < 2.4 and data[-1, 0] < 1.0
     g = tmp_path / "g.json"
@@ -90,3 +92,13 @@ def test_ingestion_matches_reference_driver(tmp_path):
     assert s.L == (L, L, L) and s.nstructures == len(ref)
     for a, b in zip(s.fibers, ref):
         np.testing.assert_array_equal(a, b[:, :4])
+
+
+def test_run_record(tmp_path):
+    from nozomi_b200.cli.simulation_main import write_run_record
+    p = tmp_path / "r.json"
+    rec = write_run_record(p, num_spins=1000, steps=500, sim_time_s=0.25, table_time_s=0.1, compartment="intra",
+                           D_final=[1.0, 2.0, 3.0])
+    assert rec["walker_steps_per_s"] == pytest.approx(2e6)
+    assert json.loads(p.read_text()) == rec
+    assert write_run_record(tmp_path / "z.json", num_spins=1, steps=1, sim_time_s=0.0)["walker_steps_per_s"] is None
