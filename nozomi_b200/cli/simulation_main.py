@@ -9,6 +9,13 @@ and a moment kernel per step).  Writes
 ``<substrate dir>/../sim/ADCdata/diffcoeff_<compartment>_<nseg>segments_<N>spins_<name>_TABLEtime<s>sec_SIMtime<s>sec_timestep<dt>ms.pkl``
 holding ``np.column_stack((Dx, Dy, Dz, t))`` as the reference does, the
 kurtoses beside it, and a JSON record of the run's timings and sizes.
+
+Two differences from the reference's loop (its simulation_main.py:90-111),
+both on purpose.  The walk takes exactly nt = int(sim_time / time_step)
+steps; the reference's float-accumulated ``current_time < nt*time_step``
+test sometimes takes one more, whose moments land past its arrays.  Row k
+holds the moments after step k + 1 at t = (k + 1) * time_step; the
+reference's saved ``diff_time[1:]`` is shifted by one step and ends in 0.
 """
 from __future__ import annotations
 

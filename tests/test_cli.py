@@ -57,6 +57,8 @@ def test_cli_end_to_end(tmp_path):
     out = list((root / "run1" / "sim" / "ADCdata").glob("diffcoeff_intra_*spins_sub_*.pkl"))
     data = pickle.load(open([p for p in out if "kurtosis" not in p.name][0], "rb"))
     assert data.shape == (500, 4)
+    # row k: D after step k + 1, at t = (k + 1) dt (aligned, unlike the reference's shifted column)
+    np.testing.assert_allclose(data[:, 3], 0.002 * np.arange(1, 501), rtol=1e-12)
     rec = json.loads(next((root / "run1" / "sim" / "ADCdata").glob("*.json")).read_text())
     assert rec["num_spins"] == 20000 and rec["steps"] == 500 and rec["walker_steps_per_s"] > 0
     # fibres along z: free along z, restricted across
