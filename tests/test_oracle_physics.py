@@ -1,4 +1,10 @@
-"""Physics of the walk rule against an analytic result, on the CPU.
+"""Physics of the walk rule against analytic results, on the CPU.
+
+The oracle is bit-exact with the reference's kernel and with the product's
+walks, so these hold for both.  Three checks: free diffusion's exp(-bD) and
+the restricted sphere's Gaussian-phase signal (the GPU versions of both run
+through the drop-in API in tests/test_dwi_physics.py), and the reference's
+own calibration target below.
 
 The reference calibrates its walker count and time step against the radial
 diffusivity inside a cylinder (tests/calibration/num_molecules_and_time_step_
@@ -56,3 +62,55 @@ def test_cylinder_radial_diffusivity_matches_burcaw():
         assert abs(D[2] / D0 - 1) < 0.05, (T, D)
     # every walker stayed inside the cylinder (containment is exact)
     assert np.hypot(spins[0], spins[1]).max() < a
+
+
+def _phase_walk(sph, nstructures, L, nseg, targets, N, D, pg, key):
+    """Oracle phase walk along x, y, z of N seeded walkers: phase [3, N]."""
+    from nozomi_b200.waveforms import step_tables
+    st, ct, it = cells_members(sph, L, nseg)
+    g = oz.Geometry(np.asarray(sph, np.float32).reshape(5, -1), nstructures, L, nseg, st, ct, it,
+                    np.full(nstructures + 1, D, np.float32), np.full(nstructures + 1, 1e9, np.float32))
+    x, _, left = oz.seed(g, targets, N, key ^ 0x5EED)
+    assert left == 0
+    G, Ga = step_tables(pg)
+    spins, spins0 = x.copy(), x.copy()
+    phase = np.zeros((3, N), np.float32)
+    oz.walk_f32(g, oz.philox(key), oz.MODE_PHASE, spins, spins0, 0, G.size, pg.dt, G=G, Garea=Ga, phase=phase,
+                diffdir=np.eye(3, dtype=np.float32), counters=False)
+    return phase
+
+
+def test_free_diffusion_signal_oracle():
+    """S(b) = exp(-b D) on an empty arena, b from the waveform's own discrete
+    sum, PGSE 20/10/30 ms at dt = 10 us: within 3 Monte Carlo standard errors
+    plus 0.2 % (the discrete b)."""
+    from nozomi_b200.waveforms import PGDiffWaveform
+    D, N = 2.0, 20_000
+    pg = PGDiffWaveform(20.0, 10.0, 30.0, time_step=0.01)
+    b1 = pg.calculate_bvalue_from_wave()
+    bvals = np.array([0.0, 0.25, 0.5, 1.0])
+    phase = _phase_walk(np.zeros((5, 0)), 0, (200.0, 200.0, 200.0), (1, 1, 1), [0], N, D, pg, 3)
+    S = oz.signal_phase(phase, np.sqrt(bvals / b1))
+    ref = np.exp(-bvals * D)
+    tol = 3 * np.sqrt(0.5 / N) + 2e-3 * ref
+    assert np.all(np.abs(S.real - ref[None, :]) <= tol[None, :]), (S.real, ref)
+    assert np.all(np.abs(S.imag) <= 3 * np.sqrt(0.5 / N) + 1e-3)
+
+
+def test_restricted_sphere_gpa_oracle():
+    """Walkers inside a sphere of radius 3 um, PGSE 20/10/30 ms: the Gaussian
+    phase approximation (Murday & Cotts 1968) at S > 0.6, averaged over x, y
+    and z, within 3 standard errors plus 1 % (the approximation)."""
+    from nozomi_b200.waveforms import PGDiffWaveform
+    from tests.test_dwi_physics import _murday_cotts
+    D, N, R = 2.0, 20_000, 3.0
+    pg = PGDiffWaveform(20.0, 10.0, 30.0, time_step=0.01)
+    amps = np.array([0.0, 0.5, 1.0, 1.5])
+    sph = np.array([[0.0], [0.0], [0.0], [R], [0.0]])
+    phase = _phase_walk(sph, 1, (10.0, 10.0, 10.0), (1, 1, 1), [0], N, D, pg, 21)
+    S = oz.signal_phase(phase, amps).real.mean(axis=0)
+    q = amps * 267.5e-4
+    delta = (pg.wave == 1).sum() * pg.dt
+    ref = np.array([_murday_cotts(qq, R - 1e-4, D, delta, 20.0) for qq in q])
+    assert np.all(ref[1:] > 0.6)
+    np.testing.assert_allclose(S, ref, atol=3 * np.sqrt(0.5 / (3 * N)) + 0.01)
