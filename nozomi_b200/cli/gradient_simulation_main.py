@@ -8,18 +8,20 @@ experiment/setup/simulation/{pgse,ogse}_sim_params.json: ``gradient.type``
 PGSE (big_delta, little_delta) or OGSE (num_oscil, duration), gradient
 ``direction`` (one [x, y, z] or a list of them), optional ``bvalues``
 (ms/um^2).  Writes the per-walker phase [ndir, N] of the unit waveform and the
-signal per (direction, b) to ``<substrate dir>/../sim/DWIdata/``.
+signal per (direction, b) to ``<substrate dir>/../sim/DWIdata/``, with a JSON
+record of the run's timings and sizes beside them.
 """
 from __future__ import annotations
 
 import os
 import pickle
+import time
 
 import numpy as np
 
 from ..diffsim3d import DwiSim3d
 from ..waveforms import ApodizedCosineOGSEWaveform, PGDiffWaveform
-from .simulation_main import build_geometry
+from .simulation_main import build_geometry, write_run_record
 
 
 def waveform(params):
@@ -56,7 +58,9 @@ def simulation_gradient_main(params, substrate_file):
         sim.setup(structures=[len(fibers)])
     else:
         sim.setup()
-    phase = sim.simulate_multi_directions(gw)
+    t0 = time.time()
+    phase = sim.simulate_multi_directions(gw)  # returns host arrays: the walk is complete
+    walk_s = time.time() - t0
     bvals = np.asarray(params.get('bvalues', [0.0, 1.0, 2.0, 3.0]), np.float64)
     amps = gw.amplitude_for_b(bvals)
     S = np.array([[np.mean(np.exp(1j * a * phase[d])) for a in amps] for d in range(dirs.shape[1])])
@@ -68,5 +72,8 @@ def simulation_gradient_main(params, substrate_file):
     with open(path, 'wb') as f:
         pickle.dump({"phase": phase, "directions": dirs, "bvalues": bvals, "signal": S,
                      "b_unit": gw.calculate_bvalue_from_wave()}, f)
+    write_run_record(os.path.splitext(path)[0] + '.json', substrate=os.path.abspath(substrate_file),
+                     compartment=compartment, num_spins=N, steps=int(len(gw.wave)), time_step_ms=float(gw.dt),
+                     nseg=nseg, directions=int(dirs.shape[1]), bvalues=bvals.tolist(), sim_time_s=float(walk_s))
     print(f"gradient simulation completed: {path}")
     return path
