@@ -54,11 +54,16 @@ class JobSpec:
 
 class SubstrateCache:
     """Device substrates (cell lists and near lists) kept resident between
-    batches, least recently used dropped first beyond ``budget_bytes``."""
+    batches, least recently used dropped first beyond ``budget_bytes``.
+
+    Callers without a key of their own pass ``id(substrate)``.  An entry
+    therefore holds its host substrate too: while the entry lives the object
+    cannot be freed, so its id cannot be reused by another substrate."""
 
     def __init__(self, budget_bytes: int = 40 << 30):
         self.budget = budget_bytes
         self.items: dict = {}
+        self.hosts: dict = {}
         self.order: list = []
         self.hits = 0
         self.misses = 0
@@ -73,10 +78,12 @@ class SubstrateCache:
         self.misses += 1
         d = device_substrate(substrate, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin)
         self.items[k] = d
+        self.hosts[k] = substrate
         self.order.append(k)
         while self.nbytes() > self.budget and len(self.order) > 1:
             old = self.order.pop(0)
             del self.items[old]
+            del self.hosts[old]
         return d
 
     def nbytes(self) -> int:

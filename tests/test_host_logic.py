@@ -93,3 +93,39 @@ def test_rebinning_kernel_count_follows_the_scan_threshold():
     assert st.sort_kernels(edge, 1, nlabels=2) == 5
     st.N = 0
     assert st.sort_kernels(packed, 8, nlabels=201) == 0
+
+
+def test_substrate_cache_lru_and_id_keys(monkeypatch):
+    """The device-substrate cache: hits, least-recently-used eviction beyond
+    its budget, and id()-keyed entries that keep their host substrate alive
+    (so a freed substrate's id cannot alias a new one while cached)."""
+    import gc
+    import weakref
+    from nozomi_b200 import batch
+    from nozomi_b200.simulate import Tuning
+
+    class FakeDevice:
+        def nbytes(self):
+            return 100
+
+    monkeypatch.setattr(batch, "device_substrate", lambda sub, **kw: FakeDevice())
+
+    class Sub:
+        pass
+
+    cache = batch.SubstrateCache(budget_bytes=250)
+    t = Tuning()
+    a, b, c = Sub(), Sub(), Sub()
+    da = cache.get(id(a), a, 2.0, 100.0, t)
+    assert cache.get(id(a), a, 2.0, 100.0, t) is da and (cache.hits, cache.misses) == (1, 1)
+    assert cache.get(id(a), a, 1.0, 100.0, t) is not da  # another D is another entry
+    ref = weakref.ref(a)
+    del a
+    gc.collect()
+    assert ref() is not None  # held by the cache while its entry lives
+    cache.get(id(b), b, 2.0, 100.0, t)  # third entry: 300 bytes > 250, the oldest goes
+    assert len(cache.items) == 2 and cache.nbytes() == 200
+    cache.get(id(c), c, 2.0, 100.0, t)
+    gc.collect()
+    assert ref() is None  # both of a's entries evicted: a is freed
+    assert set(cache.items) == set(cache.hosts)
