@@ -46,6 +46,37 @@ def signature(specs) -> str:
     return hashlib.sha1((gpu + key).encode()).hexdigest()[:16]
 
 
+def load_choices(path: Path) -> dict:
+    """Cached choices by signature; an unreadable or corrupt file is empty."""
+    try:
+        data = json.loads(Path(path).read_text())
+    except (OSError, ValueError):
+        return {}
+    return data if isinstance(data, dict) else {}
+
+
+def cached_choice(path: Path, sig: str):
+    """(Tuning, threads, entry) cached for `sig`, or None (absent, or written
+    by a version with other Tuning fields)."""
+    saved = load_choices(path).get(sig)
+    try:
+        return Tuning(**saved["tuning"]), int(saved["threads"]), saved
+    except (TypeError, KeyError, ValueError):
+        return None
+
+
+def store_choice(path: Path, sig: str, entry: dict):
+    """Add one signature's choice; the file is replaced atomically, so a
+    reader never sees it half written."""
+    path = Path(path)
+    path.parent.mkdir(parents=True, exist_ok=True)
+    data = load_choices(path)
+    data[sig] = entry
+    tmp = path.with_name(f"{path.name}.{os.getpid()}.tmp")
+    tmp.write_text(json.dumps(data, indent=1))
+    os.replace(tmp, path)
+
+
 def _trial_specs(specs, max_jobs, max_walkers, trial_steps):
     big = sorted(specs, key=lambda s: -s.walker_steps)[:max_jobs]
     out = []
@@ -77,11 +108,11 @@ def autotune(specs, space=None, trial_steps: int = 2000, max_walkers: int = 50_0
     """Returns (Tuning, threads, report)."""
     space = space or SPACE
     sig = signature(specs)
-    if use_cache and cache_file.exists():
-        saved = json.loads(cache_file.read_text()).get(sig)
-        if saved:
-            t = Tuning(**saved["tuning"])
-            return t, saved["threads"], {"cached": True, "signature": sig, **saved}
+    if use_cache:
+        hit = cached_choice(cache_file, sig)
+        if hit is not None:
+            t, threads, saved = hit
+            return t, threads, {"cached": True, "signature": sig, **saved}
     trial = _trial_specs(specs, max_jobs, max_walkers, trial_steps)
     cache = SubstrateCache()
     # start from the defaults, or a space's first value where it lacks the default
@@ -111,8 +142,6 @@ def autotune(specs, space=None, trial_steps: int = 2000, max_walkers: int = 50_0
     report = {"cached": False, "signature": sig, "tuning": dataclasses.asdict(tuning), "threads": cur["threads"],
               "trial_walker_steps_per_s": best, "trials": trials}
     if use_cache:
-        cache_file.parent.mkdir(parents=True, exist_ok=True)
-        data = json.loads(cache_file.read_text()) if cache_file.exists() else {}
-        data[sig] = {"tuning": report["tuning"], "threads": cur["threads"], "trial_walker_steps_per_s": best}
-        cache_file.write_text(json.dumps(data, indent=1))
+        store_choice(cache_file, sig, {"tuning": report["tuning"], "threads": cur["threads"],
+                                       "trial_walker_steps_per_s": best})
     return tuning, cur["threads"], report

@@ -129,3 +129,24 @@ def test_substrate_cache_lru_and_id_keys(monkeypatch):
     gc.collect()
     assert ref() is None  # both of a's entries evicted: a is freed
     assert set(cache.items) == set(cache.hosts)
+
+
+def test_autotune_choice_cache_is_robust(tmp_path):
+    """The autotuner's per-(GPU, workload) cache: a stored choice reads back
+    as the same Tuning; a corrupt file, a missing signature or an entry with
+    unknown Tuning fields is a miss, not an error; stores keep other entries."""
+    import dataclasses
+    from nozomi_b200.autotune import cached_choice, load_choices, store_choice
+    from nozomi_b200.simulate import Tuning
+    p = tmp_path / "sub" / "autotune.json"
+    assert cached_choice(p, "abc") is None
+    t = Tuning(cell=0.5, near_margin=None, steps_per_launch=2000, coarsen=8)
+    store_choice(p, "abc", {"tuning": dataclasses.asdict(t), "threads": 128, "trial_walker_steps_per_s": 1e10})
+    store_choice(p, "def", {"tuning": {"no_such_field": 1}, "threads": 64})
+    got = cached_choice(p, "abc")
+    assert got is not None and got[0] == t and got[1] == 128
+    assert cached_choice(p, "def") is None and cached_choice(p, "zzz") is None
+    assert set(load_choices(p)) == {"abc", "def"}
+    assert not list(p.parent.glob("*.tmp"))
+    p.write_text('{"abc": {"tuning": ')  # a torn write by an older version
+    assert load_choices(p) == {} and cached_choice(p, "abc") is None
