@@ -46,6 +46,16 @@ def packed_workload():
     return sub, pg, dirs, np.array([0.0, 1.0, 2.0, 3.0])
 
 
+def _store(path, obj):
+    """Pickle obj to path through a file of this process's own, renamed into
+    place: ranks that build the same cached substrate at once never see or
+    rename one another's partial files."""
+    tmp = path.with_name(f"{path.name}.{os.getpid()}.tmp")
+    with open(tmp, "wb") as f:
+        pickle.dump(obj, f)
+    os.replace(tmp, path)
+
+
 def calibration_substrate() -> Substrate:
     """A stand-in for the reference's segment-calibration substrate
     (VF0.65_d1.68_OD200_bead1.0_500axons, docs/2_calibration.md:98-108):
@@ -61,10 +71,7 @@ def calibration_substrate() -> Substrate:
             return pickle.load(f)
     s = packed_axons(n_axons=500, L=(50.0, 50.0, 50.0), spheres_per_axon=100, r_mean=0.84, r_sd=0.225,
                      bead_amp=(0.2, 0.5), bead_spacing=5.7, r_min=0.3, seed=7, max_iter=3000)
-    tmp = path.with_suffix(".tmp")
-    with open(tmp, "wb") as f:
-        pickle.dump(s, f)
-    os.replace(tmp, path)
+    _store(path, s)
     return s
 
 
@@ -76,10 +83,7 @@ def bundle(n_axons: int, seed: int) -> Substrate:
         with open(path, "rb") as f:
             return pickle.load(f)
     s = axon_bundle(n_axons, seed)
-    tmp = path.with_suffix(".tmp")
-    with open(tmp, "wb") as f:
-        pickle.dump(s, f)
-    os.replace(tmp, path)
+    _store(path, s)
     return s
 
 

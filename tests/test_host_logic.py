@@ -150,3 +150,31 @@ def test_autotune_choice_cache_is_robust(tmp_path):
     assert not list(p.parent.glob("*.tmp"))
     p.write_text('{"abc": {"tuning": ')  # a torn write by an older version
     assert load_choices(p) == {} and cached_choice(p, "abc") is None
+
+
+def _build_bundle(cache_dir, out):
+    import os
+    os.environ["NOZOMI_B200_CACHE"] = cache_dir
+    import numpy as np
+    from nozomi_b200 import workloads
+    s = workloads.bundle(12, 5)
+    np.save(out, s.spheres())
+
+
+def test_cached_substrate_built_by_several_processes_at_once(tmp_path):
+    """Ranks of one job build the same cached substrate at the same time on a
+    fresh machine: every process gets the same substrate, the cache ends with
+    one complete file and no temporary files."""
+    import multiprocessing as mp
+    import numpy as np
+    ctx = mp.get_context("spawn")
+    cache = tmp_path / "cache"
+    procs = [ctx.Process(target=_build_bundle, args=(str(cache), str(tmp_path / f"s{i}.npy"))) for i in range(3)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    arrs = [np.load(tmp_path / f"s{i}.npy") for i in range(3)]
+    assert all(np.array_equal(a, arrs[0]) for a in arrs[1:])
+    assert len(list(cache.glob("bundle_*.pkl"))) == 1 and not list(cache.glob("*.tmp"))
