@@ -259,23 +259,41 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU side
 # ---------------------------------------------------------------------------
+def _hex_id(v) -> str:
+    """A GPU UUID in comparable form: lower-case hex digits only."""
+    s = str(v).lower()
+    if s.startswith("gpu-"):
+        s = s[4:]
+    return "".join(c for c in s if c in "0123456789abcdef")
+
+
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling during the timed region.  Every GPU of the machine
+    is sampled with its UUID and PCI bus id; the summary keeps the rows of the
+    CUDA device this process runs on (nvidia-smi's index need not be CUDA's
+    under CUDA_VISIBLE_DEVICES)."""
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.path = Path("/tmp") / f"nz_clocks_{os.getpid()}.csv"
+        self.uuid, self.bus = None, None
+        try:
+            import torch
+            props = torch.cuda.get_device_properties(torch.cuda.current_device())
+            self.uuid = _hex_id(getattr(props, "uuid", "")) or None
+            self.bus = getattr(props, "pci_bus_id", None)
+        except Exception:  # device identity is a refinement; the index is the fallback
+            pass
 
     def start(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,uuid,pci.bus_id")
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.index), "-lms", "200"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
 
@@ -290,13 +308,28 @@ class Clocks:
         self.f.close()
         text = self.path.read_text()
         self.path.unlink(missing_ok=True)
-        return self.summarise(text)
+        return self.summarise(text, uuid=self.uuid, bus=self.bus, index=self.index)
 
     @staticmethod
-    def summarise(text):
+    def summarise(text, uuid=None, bus=None, index=None):
         """Median SM clock, the maximum and the throttle reasons seen in
-        nvidia-smi's csv,noheader,nounits lines (the query of start())."""
+        nvidia-smi's csv,noheader,nounits lines (the query of start()), over
+        the rows of one GPU: the one whose UUID, else PCI bus, else index
+        matches; all rows when nothing identifies it."""
         rows = [r.split(", ") for r in text.strip().splitlines() if r.strip()]
+        mine = []
+        if uuid:
+            mine = [r for r in rows if len(r) > 9 and _hex_id(r[9]) == _hex_id(uuid)]
+        if not mine and bus is not None:
+            def bus_of(r):
+                try:
+                    return int(r[10].split(":")[1], 16)
+                except (IndexError, ValueError):
+                    return None
+            mine = [r for r in rows if len(r) > 10 and bus_of(r) == int(bus)]
+        if not mine and index is not None:
+            mine = [r for r in rows if r[0].strip() == str(index)]
+        rows = mine or rows
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if len(r) > 1 and r[1].replace(".", "").isdigit()]

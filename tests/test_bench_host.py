@@ -25,6 +25,23 @@ def test_clock_summary():
     assert bench.Clocks.summarise("0, [N/A], [N/A]")["sm_mhz"] is None
 
 
+def test_clock_summary_keeps_this_gpus_rows():
+    """All GPUs are sampled; the rows kept are this CUDA device's, found by
+    UUID (any case, with or without nvidia-smi's GPU- prefix), else PCI bus,
+    else nvidia-smi index."""
+    import bench
+    tail = ", Not Active, Not Active, Not Active"
+    ours = f"3, 1950, 1965, 900.0, 0x4{tail}, Active, GPU-8d3a1c2e-aaaa-bbbb-cccc-0123456789ab, 00000000:1B:00.0"
+    other = f"0, 1200, 1965, 700.0, 0x40, Not Active, Active, Not Active, Not Active, GPU-11111111-2222-3333-4444-555555555555, 00000000:0A:00.0"
+    text = "\n".join([ours, other, ours, other, ours])
+    by_uuid = bench.Clocks.summarise(text, uuid="8D3A1C2E-AAAA-BBBB-CCCC-0123456789AB", bus=99, index=0)
+    assert by_uuid == {"sm_mhz": 1950.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    assert bench.Clocks.summarise(text, uuid=None, bus=0x1B, index=0)["samples"] == 3
+    by_index = bench.Clocks.summarise(text, index=0)
+    assert by_index["samples"] == 2 and by_index["reasons"] == ["hw_thermal_slowdown"]
+    assert bench.Clocks.summarise(text)["samples"] == 5  # nothing identifies the GPU: every row
+
+
 def test_reference_cpu_arm_runs_a_short_sample():
     """The reference arm's build (the reference's own kernel source compiled
     for the CPU, oracle/_ref) walks the packed workload's first walkers; all
