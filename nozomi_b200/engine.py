@@ -367,9 +367,21 @@ class FusedState:
         return out
 
 
+def _check_tables(who: str, step1: int, mode: int, G=None, Garea=None, moments=None):
+    """The kernels index the protocol tables and the moment rows by global
+    step; the C ABI cannot see their lengths, so they are checked here."""
+    if mode & L.MODE_PHI:
+        for name, t in (("G", G), ("Garea", Garea)):
+            if t is None or t.dtype != torch.float32 or t.numel() < step1:
+                raise NozomiError(f"{who}: {name} must be float32 with at least {step1} entries (steps to {step1})")
+    if moments is not None and (moments.dtype != torch.float64 or moments.numel() < 6 * step1):
+        raise NozomiError(f"{who}: moments must be float64 with at least {step1} rows of 6")
+
+
 def walk_fused(sub: DeviceSubstrate, st: FusedState, mode: int, dt: float, G: torch.Tensor | None,
                Garea: torch.Tensor | None, step0: int, step1: int, draws: L.Draws,
                moments: torch.Tensor | None = None):
+    _check_tables("walk_fused", int(step1), mode, G, Garea, moments if mode & L.MODE_MOMENTS else None)
     s = sub.struct()
     a = st.struct()
     L.check(L.load().nz_walk_fused(L.byref(s), L.byref(a), mode, np.float32(dt), _p(G), _p(Garea), int(step0),
@@ -381,6 +393,7 @@ def walk_fused_moments(sub: DeviceSubstrate, st: FusedState, mode: int, dt: floa
     """Steps [step0, step1) with the per-step displacement moments added to
     moments[step0:step1] ([nsteps, 6] float64).  Returns the scratch buffer
     (float32, grown as needed) for reuse."""
+    _check_tables("walk_fused_moments", int(step1), 0, moments=moments)
     lib = L.load()
     need = int(lib.nz_walk_fused_moments_scratch_bytes(st.N, int(step1) - int(step0)))
     if scratch is None or scratch.numel() * 4 < need:

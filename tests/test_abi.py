@@ -196,3 +196,24 @@ def test_invalid_arguments_rejected_without_gpu():
     # packing: walker count mismatch
     wk.spins, wk.N = FAKE, N + 1
     refused(lib.nz_state_pack(by(wk), None, by(a), None), "nz_state_pack")
+
+
+def test_protocol_tables_and_moment_rows_checked_without_gpu():
+    """The fused walk reads G / Garea and writes moment rows by global step;
+    the Python wrappers refuse tables or moment buffers that do not reach
+    step1 (or have the wrong type) before any call into the library."""
+    import torch
+    from nozomi_b200 import _lib as L
+    from nozomi_b200.engine import NozomiError, _check_tables
+    G = torch.zeros(100, dtype=torch.float32)
+    _check_tables("w", 100, L.MODE_PHI, G, G)
+    _check_tables("w", 100, 0)  # no phase: no tables needed
+    for bad in (torch.zeros(99, dtype=torch.float32), torch.zeros(100, dtype=torch.float64), None):
+        with pytest.raises(NozomiError, match="steps to 100"):
+            _check_tables("w", 100, L.MODE_PHI, G, bad)
+    m = torch.zeros((100, 6), dtype=torch.float64)
+    _check_tables("w", 100, 0, moments=m)
+    with pytest.raises(NozomiError, match="rows of 6"):
+        _check_tables("w", 101, 0, moments=m)
+    with pytest.raises(NozomiError, match="rows of 6"):
+        _check_tables("w", 10, 0, moments=m.float())
