@@ -34,7 +34,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REFERENCE_ROOT = Path(os.environ.get("NOZOMI_REFERENCE_ROOT", "/root/reference"))
+# the reference source tree: NOZOMI_REFERENCE_ROOT, else a folder named
+# "reference" beside this repository
+REFERENCE_ROOT = Path(os.environ.get("NOZOMI_REFERENCE_ROOT", HERE.parent.parent / "reference"))
 KERNEL_REL = "simulation_toolkit/simulation_engine/sim3d_kernel.cu"
 BLOCK = 1000  # DiffSim3d.set_block_grid (diffsim3d.py:170-172)
 

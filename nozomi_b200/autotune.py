@@ -11,9 +11,11 @@ in a JSON file so later runs of the same shape skip the search.
 from __future__ import annotations
 
 import dataclasses
+import fcntl
 import hashlib
 import json
 import os
+import threading
 from pathlib import Path
 
 import numpy as np
@@ -66,15 +68,23 @@ def cached_choice(path: Path, sig: str):
 
 
 def store_choice(path: Path, sig: str, entry: dict):
-    """Add one signature's choice; the file is replaced atomically, so a
-    reader never sees it half written."""
+    """Add one signature's choice.  The read-modify-write runs under an
+    exclusive lock on a sidecar file, so processes storing different
+    signatures at once keep every entry; the file is replaced atomically from
+    a temporary of this process and thread, so a reader never sees it half
+    written."""
     path = Path(path)
     path.parent.mkdir(parents=True, exist_ok=True)
-    data = load_choices(path)
-    data[sig] = entry
-    tmp = path.with_name(f"{path.name}.{os.getpid()}.tmp")
-    tmp.write_text(json.dumps(data, indent=1))
-    os.replace(tmp, path)
+    with open(path.with_name(path.name + ".lock"), "a") as lk:
+        fcntl.flock(lk.fileno(), fcntl.LOCK_EX)
+        try:
+            data = load_choices(path)
+            data[sig] = entry
+            tmp = path.with_name(f"{path.name}.{os.getpid()}.{threading.get_ident()}.tmp")
+            tmp.write_text(json.dumps(data, indent=1))
+            os.replace(tmp, path)
+        finally:
+            fcntl.flock(lk.fileno(), fcntl.LOCK_UN)
 
 
 def _trial_specs(specs, max_jobs, max_walkers, trial_steps):

@@ -6,6 +6,10 @@
 
 namespace nz {
 
+// Devices a process can drive with per-device library state (function
+// attributes, the static re-binning scratch).
+constexpr int kMaxDevices = 64;
+
 int set_error(int status, const char* fmt, ...);
 int check_launch(const char* what);
 // Host-side argument checks shared by the entry points (capi.cu): a packed

@@ -36,6 +36,7 @@
 //  * draws are counter-based (Philox at walker, step, draw), so a walker's
 //    trajectory does not depend on which thread, CTA or launch runs it.
 #include <cstdint>
+#include <mutex>
 #include "kernels.cuh"
 
 namespace nz {
@@ -163,7 +164,7 @@ __device__ __forceinline__ void jump_of(const JobDev& J, uint32_t wid, int s, in
 // in memory and are updated in place on the rare wrap / iteration-cap events
 // (except with moments, which read the origin every step).
 template <int MODE>
-__device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1, float* s_mom) {
+__device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1, double* s_mom) {
   constexpr bool kMom = (MODE & NZ_MODE_MOMENTS) != 0;
   constexpr bool kDisp = (MODE & kModeDisp) != 0;
   constexpr bool kOrig = kMom || kDisp;  // origin in registers
@@ -312,10 +313,10 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
         d[N + w] = y - y0;
         d[2 * N + w] = z - z0;
       }
-      if (kMom) {
-        const float ex = x - x0, ey = y - y0, ez = z - z0;
-        float* m = s_mom + 6 * (s - s0);
-        const float ex2 = ex * ex, ey2 = ey * ey, ez2 = ez * ez;
+      if (kMom) {  // nz_moments' terms: float displacement, squared in FP64
+        const double ex = double(x - x0), ey = double(y - y0), ez = double(z - z0);
+        double* m = s_mom + 6 * (s - s0);
+        const double ex2 = ex * ex, ey2 = ey * ey, ez2 = ez * ez;
         atomicAdd(m + 0, ex2);
         atomicAdd(m + 1, ey2);
         atomicAdd(m + 2, ez2);
@@ -351,10 +352,10 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
 // One work item: walkers [first, first + count) of job J, steps [step0, step1)
 // clamped to the job's protocol.
 template <int MODE>
-__device__ __forceinline__ void run_item(const JobDev& J, int first, int count, int step0, int step1, float* s_mom) {
+__device__ __forceinline__ void run_item(const JobDev& J, int first, int count, int step0, int step1, double* s_mom) {
   const int s0 = step0 + J.step_offset, s1 = min(step1 + J.step_offset, J.nsteps);
   if (MODE & NZ_MODE_MOMENTS) {
-    for (int i = threadIdx.x; i < kMomentSteps * 6; i += blockDim.x) s_mom[i] = 0.0f;
+    for (int i = threadIdx.x; i < kMomentSteps * 6; i += blockDim.x) s_mom[i] = 0.0;
     __syncthreads();
   }
   if (threadIdx.x < count && s0 < s1) walk_one<MODE>(J, first + threadIdx.x, s0, s1, s_mom);
@@ -362,7 +363,7 @@ __device__ __forceinline__ void run_item(const JobDev& J, int first, int count, 
     __syncthreads();
     if (J.moments)
       for (int i = threadIdx.x; i < (s1 - s0) * 6; i += blockDim.x)
-        atomicAdd(J.moments + size_t(s0) * 6 + i, double(s_mom[i]));
+        atomicAdd(J.moments + size_t(s0) * 6 + i, s_mom[i]);
     __syncthreads();
   }
 }
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
     walk_fused_kernel(const __grid_constant__ JobDev single, const nz_job* __restrict__ jobs,
                       const nz_item* __restrict__ items, int n_items, int step0, int step1, int* queue) {
   __shared__ int s_item;
-  __shared__ float s_mom[(MODE & NZ_MODE_MOMENTS) ? kMomentSteps * 6 : 1];
+  __shared__ double s_mom[(MODE & NZ_MODE_MOMENTS) ? kMomentSteps * 6 : 1];
   __shared__ JobDev s_job;
   int it = blockIdx.x;
   for (;;) {
@@ -498,12 +499,16 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
 template <int MODE>
 void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0, int step1,
                  int* queue, int grid, int threads, cudaStream_t st) {
-  // the kernel keeps no data in shared memory: give the whole carveout to L1
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(walk_fused_kernel<MODE, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    cudaFuncSetAttribute(walk_fused_kernel<MODE, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    configured = true;
+  // the kernel keeps little in shared memory: prefer the whole carveout for
+  // L1.  Function attributes belong to a device's context, so this is done
+  // once per device (and once across threads).
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) {
+    static std::once_flag once[kMaxDevices];
+    std::call_once(once[dev], [] {
+      cudaFuncSetAttribute(walk_fused_kernel<MODE, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+      cudaFuncSetAttribute(walk_fused_kernel<MODE, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    });
   }
   if (jobs)
     walk_fused_kernel<MODE, false><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);

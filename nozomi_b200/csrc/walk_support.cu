@@ -357,7 +357,6 @@ static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortScratch
 // Device address of g_sort_scratch on the current device, looked up once per
 // device (the host-side name of a __device__ array is not a device address).
 static int static_sort_scratch(void** out) {
-  constexpr int kMaxDevices = 64;
   static std::mutex mu;
   static void* addr[kMaxDevices] = {};
   int dev = 0;

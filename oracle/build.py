@@ -23,7 +23,9 @@ from pathlib import Path
 ORACLE_DIR = Path(__file__).resolve().parent
 REF_OUT = ORACLE_DIR / "_ref"
 ORACLE_SO = ORACLE_DIR / "liboracle.so"
-REFERENCE_ROOT = Path(os.environ.get("NOZOMI_REFERENCE_ROOT", "/root/reference"))
+# the reference source tree: NOZOMI_REFERENCE_ROOT, else a folder named
+# "reference" beside this repository
+REFERENCE_ROOT = Path(os.environ.get("NOZOMI_REFERENCE_ROOT", ORACLE_DIR.parent.parent / "reference"))
 REF_KERNEL_REL = "simulation_toolkit/simulation_engine/sim3d_kernel.cu"
 
 _ORACLE_SRC = [ORACLE_DIR / "walk_oracle.c", ORACLE_DIR / "walk_step.inc", ORACLE_DIR / "oz_rng.h"]

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container that holds the reference tree (default /root/reference,
-override with NOZOMI_REFERENCE_ROOT):
+Run where the reference tree is present (by default a folder named
+``reference`` beside this repository; override with NOZOMI_REFERENCE_ROOT):
 
     python tests/golden/make_golden.py [ingestion | faces]
 

@@ -9,7 +9,7 @@ per walker, different summation order).
 import numpy as np
 import pytest
 
-from tests._fixtures import DWI, NARROW, dirs_of, load, oracle_geometry
+from tests._fixtures import DWI, EDGE, NARROW, dirs_of, load, oracle_geometry
 from oracle import oracle as oz
 from oracle.cells_oracle import cells_members, segments_reference
 
@@ -96,7 +96,7 @@ def test_plain_narrow_matches_reference(eng, name):
     np.testing.assert_array_equal(wk.flags.cpu().numpy(), r["flags"])
 
 
-@pytest.mark.parametrize("name", DWI)
+@pytest.mark.parametrize("name", DWI + EDGE)
 def test_plain_dwi_matches_reference(eng, name):
     c = load(name)
     sub = _sub_from_case(eng, c)
@@ -114,7 +114,7 @@ def test_plain_dwi_matches_reference(eng, name):
     np.testing.assert_array_equal(wk.phase.cpu().numpy(), c["phase"])
 
 
-@pytest.mark.parametrize("name", DWI + NARROW[:2])
+@pytest.mark.parametrize("name", DWI + EDGE + NARROW[:2])
 def test_fused_matches_oracle_and_reference(eng, name):
     """The fused kernel (one launch for all steps, Phi form) against the oracle
     with the same cell lists: positions, spins0, labels and Phi bit-exact; and
@@ -275,7 +275,7 @@ def test_signal_and_moments_match_oracle(eng):
 
 
 @pytest.mark.parametrize("name,margin", [("dwi_c1_cells", 0.5), ("dwi_c1_cells", 0.25), ("dwi_overlap", 0.4),
-                                         ("narrow_periodic_in", 0.3)])
+                                         ("narrow_periodic_in", 0.3), ("dwi_faces", 0.3), ("dwi_faces", 0.6)])
 def test_fused_near_lists_match_full_lists(eng, name, margin):
     """Near lists (smaller margin, used when an iteration's reach fits) give
     the full lists' result bit for bit: the fused walk with near lists against
@@ -310,11 +310,11 @@ def test_fused_near_lists_match_full_lists(eng, name, margin):
 
 
 def test_fused_moments_equal_per_step_moments(eng):
-    """Narrow-pulse moments accumulated inside the fused walk (lanes of a warp
-    in lock-step, warp shuffle sums) against the plain walk with one moment
-    reduction per step (computeDiffusionCoefficientsAndKurtosis's role,
+    """Narrow-pulse moments accumulated inside the fused walk (per-CTA FP64
+    shared-memory sums of nz_moments' terms) against the plain walk with one
+    moment reduction per step (computeDiffusionCoefficientsAndKurtosis's role,
     sim3d_kernel.cu:162-238): identical trajectories, per-step sums equal to
-    float summation order.  3001 walkers leave partial warps; 300 steps span
+    FP64 summation order.  3001 walkers leave partial warps; 300 steps span
     two launches."""
     from nozomi_b200 import _lib as L
     from nozomi_b200.simulate import device_substrate
@@ -345,7 +345,7 @@ def test_fused_moments_equal_per_step_moments(eng):
     torch.cuda.synchronize()
     np.testing.assert_array_equal(out.spins.cpu().numpy(), wk.spins.cpu().numpy())
     np.testing.assert_array_equal(out.sig.cpu().numpy(), wk.sig.cpu().numpy())
-    np.testing.assert_allclose(fused.cpu().numpy(), per_step.cpu().numpy(), rtol=2e-5, atol=0)
+    np.testing.assert_allclose(fused.cpu().numpy(), per_step.cpu().numpy(), rtol=1e-12, atol=0)
     # the displacement form (nz_walk_fused_moments): every term is nz_moments',
     # so the sums agree to FP64 summation order; any number of steps per call
     w3 = eng.Walkers(x0.clone(), x0.clone(), sig=torch.ones(N, device="cuda"), label=lab.clone(),

@@ -152,6 +152,30 @@ def test_autotune_choice_cache_is_robust(tmp_path):
     assert load_choices(p) == {} and cached_choice(p, "abc") is None
 
 
+def _store_many(path, tag, n):
+    from nozomi_b200.autotune import store_choice
+    for i in range(n):
+        store_choice(path, f"{tag}-{i}", {"tuning": {}, "threads": 128})
+
+
+def test_autotune_stores_from_several_processes_keep_every_entry(tmp_path):
+    """Four processes each store 15 different signatures into one cache file
+    at the same time: the locked read-modify-write keeps all 60 entries and
+    leaves no temporary or half-written file."""
+    import multiprocessing as mp
+    from nozomi_b200.autotune import load_choices
+    ctx = mp.get_context("spawn")
+    p = tmp_path / "autotune.json"
+    procs = [ctx.Process(target=_store_many, args=(str(p), f"p{k}", 15)) for k in range(4)]
+    for q in procs:
+        q.start()
+    for q in procs:
+        q.join(120)
+        assert q.exitcode == 0
+    assert set(load_choices(p)) == {f"p{k}-{i}" for k in range(4) for i in range(15)}
+    assert not list(tmp_path.glob("*.tmp"))
+
+
 def _build_bundle(cache_dir, out):
     import os
     os.environ["NOZOMI_B200_CACHE"] = cache_dir
