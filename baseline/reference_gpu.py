@@ -183,8 +183,15 @@ BUILDS = {  # name: what it is
 }
 
 
+# jobs of the batched mixed workload (mixed_specs(seed=4), 64 jobs) whose
+# substrates the reference arm of the batched benchmark walks: one of every 16
+BATCH_SAMPLE_JOBS = (0, 16, 32, 48)
+
+
 def workload_pars(name: str, nspins: int | None = None) -> dict:
-    """Template pars of a named workload (walker count overridable)."""
+    """Template pars of a named workload (walker count overridable):
+    packed_1e6, single_axon_1e4, or batched_job<i> (job i of the batched
+    mixed workload, 1 um cells)."""
     from nozomi_b200.substrates import beaded_axon, cell_grid
     if name == "packed_1e6":
         from nozomi_b200.workloads import packed_workload
@@ -192,6 +199,10 @@ def workload_pars(name: str, nspins: int | None = None) -> dict:
         nseg, N = cell_grid(sub.L, 1.0), 1_000_000
     elif name == "single_axon_1e4":
         sub, nseg, N = beaded_axon(), (1, 1, 8), 10_000
+    elif name.startswith("batched_job"):
+        from nozomi_b200.workloads import mixed_specs
+        sp = mixed_specs(seed=4, n_jobs=64)[int(name[len("batched_job"):])]
+        sub, nseg, N = sp.substrate, cell_grid(sp.substrate.L, 1.0), sp.N
     else:
         raise KeyError(name)
     N = N if nspins is None else int(nspins)

@@ -1,30 +1,52 @@
-"""Benchmark of the spin random walk: walker-steps/s on the packed-substrate
-workload (200 beaded axons, 20,000 spheres + periodic images, 40x40x80 um box,
-1e6 walkers per GPU, PGSE 20/10/30 ms at dt = 5 us = 6000 steps, 30 directions
-x b in {0, 1, 2, 3} ms/um^2).
+"""Benchmark of the spin random walk: walker-steps/s on one B200.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload batched|packed|serving|narrow]
 
-One step = one pass of the hot path over one batch: every walker through all
-6000 time steps (fused launches with re-binning between them) plus the signal
-reduction, inputs (seeded positions, substrate, protocol) resident in HBM.
-`value` is the whole-job walker-steps/s (all ranks; walkers are sharded,
-weak scaling, no data-path collective).  `e2e` is the same metric through the
-public call with host buffers: positions copied in from pinned memory and the
-signal copied out every step.
+Default workload (``batched``): the mixed workload the headline metric is
+quoted on -- 64 independent substrates of 10-500 beaded axons, walker counts
+log-uniform in [1e4, 1e6], 2000-8000 steps at dt = 5 us, per-substrate PGSE
+protocols with 6-60 directions, b in {0, 1, 2, 3} ms/um^2 (seed 4) -- walked
+together by the batched persistent work-queue kernel, the whole step captured
+as a CUDA graph.  One step = every walker of every job through all of its
+steps plus the signal reductions, inputs resident in HBM.  Beside `value` the
+line reports:
+
+  plain            the plain per-substrate path (one kernel launch per
+                   waveform sample, per-direction phase in HBM, jobs one after
+                   another) on every k-th job, and speedup_vs_plain;
+  serving          the same distribution as Poisson request streams through
+                   the continuous-batching server: p50/p99 latency and served
+                   walker-steps/s per rate (5 and 20 req/s, stated windows);
+  e2e              the same workload through the public batched call
+                   (nozomi_b200.batch.simulate_batch) with positions in pinned
+                   host memory and the signals copied back, every step;
+  roofline         the dominant kernel's issue roofline (ncu-counted warp
+                   instructions per walker-step x kernel walker-steps/s over
+                   4 issue slots x SMs x clock), with the kernel-source hash
+                   the counts were taken on; FP32 and HBM views beside it;
+  cpu_baseline     the reference's own kernel compiled for the host cores on a
+                   bounded sample of the same jobs.
 
 --impl reference: the reference has no CPU implementation of the walk; the
 reference arm times the reference's own kernel source compiled for the CPU
 (oracle/_ref, built where the reference tree is present: its launches run as
 OpenMP loops over walkers on the host cores) on a bounded sample of the same
-workload, or, without that build, the oracle's C restatement of the kernel.
---impl reference_gpu: the reference's kernel compiled for sm_100a (baseline/_ref)
-launched on this GPU one waveform sample at a time, as the reference does.
+workload's jobs, or, without that build, the oracle's C restatement of the
+kernel.  --impl reference_gpu: the reference's kernel compiled for sm_100a
+(baseline/_ref) launched on this GPU one waveform sample at a time, as the
+reference does (packed workload).
+
+--workload packed: one packed substrate (200 beaded axons, 20,000 spheres +
+periodic images, 40x40x80 um box, 1e6 walkers per GPU, PGSE 20/10/30 ms at
+dt = 5 us = 6000 steps, 30 directions x b in {0, 1, 2, 3} ms/um^2) through the
+single-substrate fused walk.  --workload serving: the request streams alone.
+--workload narrow: the narrow-pulse simulation CLI path.
 """
 from __future__ import annotations
 
 import argparse
 import dataclasses
+import hashlib
 import json
 import os
 import subprocess
@@ -40,29 +62,53 @@ sys.path.insert(0, str(ROOT))
 WORKLOAD = ("packed substrate: 200 beaded axons x 100 spheres (lognormal r0 1.0/0.3 um, bead amplitude "
             "U[0.2,0.5]), periodic 40x40x80 um box, 1e6 walkers/GPU over intra+extra space, D=2.0 um^2/ms, "
             "PGSE delta=10 Delta=20 te=30 ms at dt=5 us (6000 steps), 30 directions x b={0,1,2,3} ms/um^2")
+BATCH_WORKLOAD = ("batched mixed workload: {jobs} substrates of 10-500 beaded axons (40 spheres at 1 um, radii "
+                  "U[0.5,1.5], z-periodic, packed at area fraction 0.35), walkers log-uniform 1e4-1e6 (x{scale}), "
+                  "2000-8000 steps at dt=5 us (PGSE delta=te/3, Delta=2te/3), 6-60 directions, b={{0,1,2,3}} "
+                  "ms/um^2, seed 4; all jobs in persistent work-queue launches under one CUDA graph")
+
+# The fused walk's source files: the instruction and DRAM counts below hold
+# for the kernel built from exactly these sources (sha1 of their bytes).
+KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.cuh", "nozomi_b200/csrc/kernels.cuh")
+
+# Per workload, from one ncu capture of walk_fused_kernel (--set full,
+# --clock-control none) on a small case of that workload: warp instructions
+# executed (smsp__inst_executed.sum) and DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum) of the captured launch, divided by the walker-steps
+# that launch ran; kernel_sha: the sources' hash at capture.
+PROFILED = {
+    "packed": {"kernel_sha": None, "warp_inst_per_walker_step": None, "dram_bytes_per_walker_step": None,
+               "capture": None},
+    "batched": {"kernel_sha": None, "warp_inst_per_walker_step": None, "dram_bytes_per_walker_step": None,
+                "capture": None},
+}
 
 
-# the configuration profiled with ncu, its DRAM read + write bytes per
-# walk_fused_kernel launch (1e6 walkers x 2000 steps) and its warp
-# instructions per walker-step
-PROFILED_SHAPE = (1_000_000, 0.5, 0.5, 2000)
-PROFILED_TRAFFIC_BYTES = 9_966_812_000 + 94_345_472
-PROFILED_WARP_INST_PER_WALKER_STEP = 56.5
+def kernel_sha() -> str:
+    h = hashlib.sha1()
+    for rel in KERNEL_SOURCES:
+        h.update((ROOT / rel).read_bytes())
+    return h.hexdigest()[:16]
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference_gpu"],
                     help="reference: the reference's walk on the host cores; reference_gpu: the reference's own "
                          "CUDA kernel (baseline/_ref build) on this GPU, one launch per waveform sample")
+    ap.add_argument("--workload", default="batched", choices=["batched", "packed", "serving", "narrow"],
+                    help="batched: 64 mixed substrates in persistent batched launches (default); packed: one "
+                         "packed substrate; serving: Poisson request streams alone; narrow: the narrow-pulse "
+                         "simulation CLI path on a calibration-like substrate")
     ap.add_argument("--ref-samples", type=int, default=600,
                     help="reference_gpu: waveform samples (launches) timed, after --warmup x 10 untimed")
-    ap.add_argument("--walkers", type=int, default=1_000_000)
+    ap.add_argument("--walkers", type=int, default=1_000_000, help="packed: walkers per GPU")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0,
+                    help="target CPU work of the CPU baseline sample (and of each reference-arm step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cell", type=float, default=None)
     ap.add_argument("--steps-per-launch", type=int, default=None)
@@ -71,24 +117,82 @@ def parse():
     ap.add_argument("--near-margin", type=float, default=None, help="near-list margin in um (0: none)")
     ap.add_argument("--narrow-walkers", type=float, default=5e5, help="narrow: walkers")
     ap.add_argument("--narrow-ms", type=float, default=100.0, help="narrow: simulated time, ms")
-    ap.add_argument("--workload", default="packed", choices=["packed", "batched", "serving", "narrow"],
-                    help="packed: one packed substrate (default); batched: 64 mixed substrates, batched vs plain; "
-                         "serving: Poisson request streams, continuous batching, p50/p99 latency; "
-                         "narrow: the narrow-pulse simulation CLI path on a calibration-like substrate")
-    ap.add_argument("--rates", default="5,20,50,100,200", help="serving: request rates (req/s)")
-    ap.add_argument("--serve-seconds", type=float, default=20.0, help="serving: arrival window per rate")
-    ap.add_argument("--serve-cell", type=float, default=1.5, help="serving: cell edge of the cached lists, um")
-    ap.add_argument("--serve-coarsen", type=int, default=8, help="serving: re-binning bins in cells per axis")
-    ap.add_argument("--max-requests", type=int, default=200, help="serving: requests per rate at most")
+    ap.add_argument("--serve", default="5:30,20:10",
+                    help="serving: rate:window pairs, requests per second and seconds of arrivals")
+    ap.add_argument("--no-serving", action="store_true", help="batched: skip the serving leg")
+    ap.add_argument("--serve-cell", type=float, default=None, help="serving: cell edge of the cached lists, um")
+    ap.add_argument("--serve-coarsen", type=int, default=None, help="serving: re-binning bins in cells per axis")
+    ap.add_argument("--max-requests", type=int, default=None, help="serving: requests per rate at most")
     ap.add_argument("--jobs", type=int, default=64, help="batched: number of substrates")
     ap.add_argument("--walker-scale", type=float, default=1.0, help="batched: scale of the walker counts")
     ap.add_argument("--threads", type=int, default=128, help="batched: walkers per CTA")
-    ap.add_argument("--plain-every", type=int, default=1, help="batched: time the plain path on every k-th job")
+    ap.add_argument("--plain-every", type=int, default=4, help="batched: time the plain path on every k-th job")
+    ap.add_argument("--no-plain", action="store_true", help="batched: skip the plain-path comparison")
     ap.add_argument("--autotune", action="store_true", help="batched: pick the launch shape with the autotuner")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
-def workload():
+def load_peaks():
+    """MEASURED_PEAKS.json of this machine (hbm_gbs, bf16_tflops, ...), or {}."""
+    pk = ROOT / "MEASURED_PEAKS.json"
+    return (json.loads(pk.read_text()), "MEASURED_PEAKS.json") if pk.exists() else ({}, None)
+
+
+def rooflines(workload: str, kernel_ws_s: float, ws_per_launch: float, launch_ms: float, state_bytes: float,
+              clk, sms: int, fp32_peak_tflops: float, f_alg: float | None, work=None):
+    """The dominant kernel's rooflines: issue (the binding one), FP32 and HBM.
+    kernel_ws_s: its walker-steps per second of kernel time; ws_per_launch:
+    walker-steps of an average launch; state_bytes: algorithmic bytes of an
+    average launch (walker state in and out)."""
+    prof = PROFILED.get(workload, {})
+    sha = kernel_sha()
+    stale = prof.get("kernel_sha") != sha
+    peaks, src = load_peaks()
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    issue = None
+    wi = prof.get("warp_inst_per_walker_step")
+    if wi:
+        peak = sms * 4 * mhz * 1e6
+        ach = wi * kernel_ws_s
+        db = prof.get("dram_bytes_per_walker_step")
+        issue = {"bound": "issue", "achieved": ach, "peak": peak, "unit": "warp-instructions/s",
+                 "frac": ach / peak, "warp_instructions_per_walker_step": wi,
+                 "traffic": None if db is None else db * ws_per_launch,
+                 "traffic_scaling": "DRAM bytes per walker-step of the captured launch x walker-steps of an "
+                                    "average launch here",
+                 "peak_source": f"{sms} SMs x 4 issue slots x median SM clock under load ({mhz:.0f} MHz)",
+                 "counts_kernel_sha": prof.get("kernel_sha"), "kernel_sha": sha, "stale": stale,
+                 "capture": prof.get("capture")}
+    fp32 = None
+    if f_alg is not None:
+        ach = kernel_ws_s * f_alg / 1e12
+        fp32 = {"bound": "fp32", "achieved": ach, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
+                "frac": ach / fp32_peak_tflops, "flops_per_walker_step": f_alg, "work_per_walker_step": work,
+                "peak_source": "nz_probe_fma on this GPU (8 FFMA chains per thread)"}
+    hbm = {"bound": "hbm", "achieved": state_bytes / (launch_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+           "algorithmic_bytes_per_launch": state_bytes,
+           "peak_source": f"{src} hbm_gbs" if src else "fallback 6.65 TB/s"}
+    hbm["frac"] = hbm["achieved"] / hbm_peak
+    return issue, fp32, hbm
+
+
+def fp32_peak(lib, L, stream, sms):
+    """FP32 FMA throughput of this GPU (TFLOP/s) from the probe kernel."""
+    import torch
+    out = torch.zeros(sms * 16, device="cuda")
+    iters = 4096
+    for _ in range(2):
+        L.check(lib.nz_probe_fma(sms * 16, iters, out.data_ptr(), stream.cuda_stream), "probe")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    L.check(lib.nz_probe_fma(sms * 16, iters, out.data_ptr(), stream.cuda_stream), "probe")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return sms * 16 * 256 * iters * 8 * 2 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+
+def workload_packed():
     from nozomi_b200.workloads import packed_workload
     return packed_workload()
 
@@ -97,8 +201,11 @@ def workload():
 # CPU side: the oracle on the host cores
 # ---------------------------------------------------------------------------
 def cpu_sample(sub, pg, dirs, cell, seconds, rank_seed=0, work=True):
-    """Time the oracle on a bounded sample sized to about `seconds` of work.
-    Returns (walker-steps/s, cores, sample description, work per walker-step)."""
+    """Time the oracle (the C restatement, OpenMP over walkers) on a bounded
+    sample of one substrate and protocol, sized to about `seconds` of work.
+    Returns (walker-steps/s, cores, sample description, work per walker-step:
+    iterations, spheres and solves within reach, from the oracle's count
+    mode on up to 2048 walkers x 200 steps)."""
     from oracle import oracle as oz
     from nozomi_b200.substrates import cell_grid
     from nozomi_b200.waveforms import step_tables
@@ -140,7 +247,6 @@ def cpu_sample(sub, pg, dirs, cell, seconds, rank_seed=0, work=True):
     return value, cores, sample, wk
 
 
-REF_CPU_BUILD = "packed_cpu_16k"
 REF_CPU_KIND = ("the reference's own sim3d_kernel.cu (randomWalk3d_phase_multidirr, template filled as DiffSim3d "
                 "does, padded set_segments table at 1 um cells) compiled for the CPU with host stand-ins for its "
                 "CUDA headers (oracle/refshim): each kernel launch runs its 1000-thread blocks as OpenMP "
@@ -148,16 +254,17 @@ REF_CPU_KIND = ("the reference's own sim3d_kernel.cu (randomWalk3d_phase_multidi
 
 
 class ReferenceCpu:
-    """The reference kernel's CPU build (oracle/_ref, named build) walking
-    the first N walkers of the packed workload, launch by launch."""
+    """A named CPU build of the reference kernel (oracle/_ref) walking its
+    walkers (seeded over the whole substrate) through a protocol, launch by
+    launch, as DwiSim3d.simulate_multi_directions does."""
 
-    def __init__(self, sub, pg, dirs, key=1000):
+    def __init__(self, build: str, sub, gwave, dirs, key=1000):
         import ctypes
         from oracle import oracle as oz
         from oracle.build import reference_named
-        b = reference_named(REF_CPU_BUILD)
+        b = reference_named(build)
         if b is None:
-            raise FileNotFoundError(f"oracle/_ref build {REF_CPU_BUILD} is absent")
+            raise FileNotFoundError(f"oracle/_ref build {build} is absent")
         so, pars = b
         self.lib = ctypes.CDLL(str(so))
         P, f, i = ctypes.c_void_p, ctypes.c_float, ctypes.c_int
@@ -169,7 +276,7 @@ class ReferenceCpu:
         self.N = N = int(pars["nspins"])
         nseg = cell_grid(sub.L, 1.0)
         if (int(pars["nLx"]), int(pars["nLy"]), int(pars["nLz"])) != tuple(nseg) or int(pars["nspheres"]) != sub.S:
-            raise ValueError("the reference CPU build does not match this workload")
+            raise ValueError(f"the reference CPU build {build} does not match this substrate")
         sph64 = sub.spheres()
         st, ct, it = oz.cells(sph64, sub.L, nseg)
         self.K = K = int(pars["nspheres_per_seg"])
@@ -185,9 +292,9 @@ class ReferenceCpu:
         self.ndir = dirs.shape[1]
         self.phase = np.zeros(self.ndir * N, np.float32)
         self.sph = np.ascontiguousarray(sph64.astype(np.float32))
-        self.dd = np.ascontiguousarray(dirs.astype(np.float32))
-        self.G, self.Ga = step_tables(pg)
-        self.dt = float(pg.dt)
+        self.dd = np.ascontiguousarray(np.asarray(dirs, np.float32))
+        self.G, self.Ga = step_tables(gwave)
+        self.dt = float(gwave.dt)
         self.lib.ref_run_initstates(N // 1000, 1000, 1000)
         self.lib.ref_set_philox(key, 0, 0)
         self.n = 0
@@ -204,53 +311,82 @@ class ReferenceCpu:
             self.n += 1
 
 
-def reference_cpu_sample(sub, pg, dirs, seconds, steps=1, warmup=0):
-    """Time the reference kernel's CPU build: `warmup` + `steps` samples of
-    about `seconds` each.  Returns (walker-steps/s, cores, sample text, ms per
-    timed sample)."""
+def reference_cases(workload: str):
+    """(build name, substrate, waveform, directions) the reference arm walks:
+    the packed workload, or jobs 0, 16, 32, 48 of the batched mixed workload."""
+    if workload == "packed":
+        sub, pg, dirs, _ = workload_packed()
+        return [("packed_cpu_16k", sub, pg, dirs)], "the packed workload"
+    from baseline.reference_gpu import BATCH_SAMPLE_JOBS
+    from nozomi_b200.workloads import mixed_specs
+    specs = mixed_specs(seed=4, n_jobs=64)
+    cases = [(f"batched_job{i}_cpu_8k", specs[i].substrate, specs[i].gwave, np.asarray(specs[i].dirs))
+             for i in BATCH_SAMPLE_JOBS]
+    return cases, f"jobs {', '.join(map(str, BATCH_SAMPLE_JOBS))} of the batched workload"
+
+
+def reference_cpu_sample(cases, seconds, steps=1, warmup=0):
+    """Time the reference kernel's CPU builds: per step, every case for about
+    seconds / len(cases).  Returns (walker-steps/s, cores, sample text, ms
+    per timed step)."""
     cores = os.cpu_count() or 1
-    r = ReferenceCpu(sub, pg, dirs)
+    refs = [ReferenceCpu(b, sub, gw, dirs) for b, sub, gw, dirs in cases]
+    per = []
+    for r in refs:
+        t = time.perf_counter()
+        r.run(3)
+        rate = r.N * 3 / (time.perf_counter() - t)
+        per.append(int(np.clip(seconds / len(refs) * rate / r.N, 3, r.G.size)))
+    for r, k in zip(refs, per):
+        r.run(k * warmup)
     t = time.perf_counter()
-    r.run(5)
-    rate = r.N * 5 / (time.perf_counter() - t)
-    per = int(np.clip(seconds * rate / r.N, 5, r.G.size))
-    r.run(per * warmup)
-    t = time.perf_counter()
-    r.run(per * steps)
+    for _ in range(steps):
+        for r, k in zip(refs, per):
+            r.run(k)
     el = time.perf_counter() - t
-    sample = (f"{r.N} walkers x {per} launches per step x {steps} step(s) (waveform samples "
-              f"{5 + per * warmup}..{5 + per * (warmup + steps) - 1}), {el:.1f} s, padded K={r.K}")
-    return r.N * per * steps / el, cores, sample, el * 1e3 / steps
+    ws = steps * sum(r.N * k for r, k in zip(refs, per))
+    sample = "; ".join(f"{b}: {r.N} walkers x {k} launches per step, padded K={r.K}"
+                       for (b, *_), r, k in zip(cases, refs, per))
+    return ws / el, cores, f"{sample}; {steps} step(s), {el:.1f} s", el * 1e3 / steps
+
+
+def port_sample(cases, seconds, cell=1.0, steps=1, warmup=0):
+    """The oracle's C restatement on the same cases (no reference build)."""
+    total_t, total_ws, texts, cores = 0.0, 0, [], 1
+    for i in range(warmup + steps):
+        for _, sub, gw, dirs in cases:
+            v, cores, sample, _ = cpu_sample(sub, gw, dirs, cell, seconds / len(cases), rank_seed=i, work=False)
+            if i >= warmup:
+                total_ws += 1
+                total_t += 1.0 / v
+                texts.append(sample)
+    return total_ws / total_t, cores, "; ".join(texts[:len(cases)])
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sub, pg, dirs, bvals = workload()
+    workload = "packed" if args.workload == "packed" else "batched"
+    cases, what = reference_cases(workload)
     from oracle.build import build_oracle
     build_oracle()
     try:
-        value, cores, sample, ms_step = reference_cpu_sample(sub, pg, dirs, args.cpu_seconds / 2, steps=args.steps,
+        value, cores, sample, ms_step = reference_cpu_sample(cases, args.cpu_seconds / 2, steps=args.steps,
                                                              warmup=args.warmup)
         kind, how = "reference", REF_CPU_KIND
     except (FileNotFoundError, ValueError) as e:  # no reference build on this host: the C restatement
-        total_t, total_ws = 0.0, 0
-        for i in range(args.warmup + args.steps):
-            v, cores, sample, _ = cpu_sample(sub, pg, dirs, args.cell or 1.0, args.cpu_seconds / 2, rank_seed=i,
-                                             work=False)
-            if i >= args.warmup:
-                total_ws += 1
-                total_t += 1.0 / v
-        value = total_ws / total_t
+        value, cores, sample = port_sample(cases, args.cpu_seconds / 2, steps=args.steps, warmup=args.warmup)
         ms_step = None  # samples of differing walker counts: no common step time
         kind, how = "port", f"oracle/walk_oracle.c, the C restatement of the kernel, OpenMP over walkers ({e})"
+    wl = WORKLOAD if workload == "packed" else BATCH_WORKLOAD.format(jobs=args.jobs, scale=args.walker_scale)
     line = {"impl": "reference", "metric": "walker-steps/s", "value": value, "unit": "walker-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cell_um": 1.0},
+            "higher_is_better": True, "scaling": "weak" if workload == "packed" else "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl, "cell_um": 1.0, "sampled": what},
             "cpu_baseline": {"value": value, "unit": "walker-steps/s", "cores": cores, "kind": kind,
-                             "sample": sample + "; " + how},
+                             "sample": f"{what}: {sample}; {how}"},
             "e2e": {"value": value, "unit": "walker-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -340,7 +476,7 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def run_ours(args):
+def run_packed(args):
     import torch
     import torch.distributed as dist
     from nozomi_b200 import engine, _lib as L
@@ -358,9 +494,9 @@ def run_ours(args):
         from nozomi_b200.shard import init_process_group
         init_process_group("nccl", timeout_s=180)
     engine.require_cuda()
-    sub, pg, dirs, bvals = workload()
-    # launch shape tuned for this workload (profiles/walk_fused_packed_tuning.md):
-    # 0.5 um cells, near margin 0.5 um, re-binning bins of 8^3 cells, 2000 steps per launch
+    sub, pg, dirs, bvals = workload_packed()
+    # launch shape tuned for this workload by sweeps on a B200: 0.5 um cells,
+    # near margin 0.5 um, re-binning bins of 8^3 cells, 2000 steps per launch
     tuning = Tuning(cell=0.5, near_margin=0.5, coarsen=8, steps_per_launch=2000)
     if args.cell:
         tuning.cell = args.cell
@@ -404,17 +540,8 @@ def run_ours(args):
 
     # FP32 peak of this GPU (probe kernel), before the timed region
     sms = torch.cuda.get_device_properties(local).multi_processor_count
-    probe_out = torch.zeros(sms * 16, device="cuda")
     lib = L.load()
-    iters = 4096
-    for _ in range(2):
-        L.check(lib.nz_probe_fma(sms * 16, iters, probe_out.data_ptr(), stream.cuda_stream), "probe")
-    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    pe0.record(stream)
-    L.check(lib.nz_probe_fma(sms * 16, iters, probe_out.data_ptr(), stream.cuda_stream), "probe")
-    pe1.record(stream)
-    torch.cuda.synchronize()
-    fp32_peak_tflops = sms * 16 * 256 * iters * 8 * 2 / (pe0.elapsed_time(pe1) * 1e-3) / 1e12
+    fp32_peak_tflops = fp32_peak(lib, L, stream, sms)
 
     for _ in range(args.warmup):
         one_step()
@@ -509,44 +636,17 @@ def run_ours(args):
             port = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "port",
                     "sample": sample + "; oracle/walk_oracle.c, OpenMP over walkers"}
             try:
-                v, cores, sample, _ = reference_cpu_sample(sub, pg, dirs, args.cpu_seconds / 2)
+                v, cores, sample, _ = reference_cpu_sample(reference_cases("packed")[0], args.cpu_seconds / 2)
                 cpu = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "reference",
                        "sample": sample + "; " + REF_CPU_KIND, "port": port}
             except (FileNotFoundError, ValueError) as e:
                 cpu = dict(port, reference_unavailable=str(e))
-        peaks = {}
-        pk = ROOT / "MEASURED_PEAKS.json"
-        if pk.exists():
-            peaks = json.loads(pk.read_text())
-        hbm_peak = peaks.get("hbm_gbs", 6650.0)
-        # HBM view: walker state read + written once per launch (4 x float4 each way)
-        state_bytes = N * 128
-        # DRAM bytes of one launch from an ncu capture of this configuration
-        # (profiles/walk_fused_packed1e6_ncu.md); none for other shapes
-        traffic = None
-        if (N, tuning.cell, tuning.near_margin, tuning.steps_per_launch) == PROFILED_SHAPE:
-            traffic = PROFILED_TRAFFIC_BYTES
-        roof_hbm = {"bound": "hbm", "achieved": state_bytes / (walk_launch_ms * 1e-3) / 1e9, "peak": hbm_peak,
-                    "unit": "GB/s", "traffic": traffic, "algorithmic_bytes_per_launch": state_bytes,
-                    "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk.exists() else "fallback 6.65 TB/s"}
-        roof_hbm["frac"] = roof_hbm["achieved"] / hbm_peak
-        roof_fp32 = None
+        F_alg = None
         if wk is not None:
             F_alg = 10 * wk["spheres_in_reach"] + 36 * wk["solves_in_reach"] + 6 * dirs.shape[1]
-            ach = kernel_ws_s * F_alg / 1e12
-            roof_fp32 = {"bound": "fp32", "achieved": ach, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
-                         "frac": ach / fp32_peak_tflops, "flops_per_walker_step": F_alg, "work_per_walker_step": wk,
-                         "peak_source": "nz_probe_fma on this GPU (8 FFMA chains/thread)"}
-        # the bound that binds this kernel: instruction issue (4 warp-instructions
-        # per SM per cycle), with the warp-instructions per walker-step counted
-        # by ncu for the profiled shape
-        roof_issue = None
-        if traffic is not None and clk and clk.get("sm_mhz"):
-            peak = sms * 4 * clk["sm_mhz"] * 1e6
-            ach = PROFILED_WARP_INST_PER_WALKER_STEP * kernel_ws_s
-            roof_issue = {"bound": "issue", "achieved": ach, "peak": peak, "unit": "warp-instructions/s",
-                          "frac": ach / peak, "warp_instructions_per_walker_step": PROFILED_WARP_INST_PER_WALKER_STEP,
-                          "peak_source": f"{sms} SMs x 4 issue slots x median SM clock under load"}
+        # walker state read and written once per launch (4 x float4 each way)
+        roof_issue, roof_fp32, roof_hbm = rooflines("packed", kernel_ws_s, per_launch_ws, walk_launch_ms, N * 128,
+                                                    clk, sms, fp32_peak_tflops, F_alg, wk)
         line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -572,7 +672,7 @@ def run_ours(args):
                 "cell_build": {"ms": cell_build_ms, "timing": "wall clock of one device_substrate build "
                                "(host preparation, cell and near lists, per-entry records), synchronised on "
                                "both sides; once per substrate, not part of value"},
-                "roofline": roof_hbm, "roofline_fp32": roof_fp32, "roofline_issue": roof_issue,
+                "roofline": roof_issue, "roofline_fp32": roof_fp32, "roofline_hbm": roof_hbm,
                 "cpu_baseline": cpu, "clocks": clk,
                 "signal_b0_mean": float(np.mean(np.abs(S[:, 0]))),
                 "signal_mean_by_b": [float(np.mean(S[:, b].real)) for b in range(S.shape[1])]}
@@ -583,56 +683,140 @@ def run_ours(args):
     return 0
 
 
-BATCH_WORKLOAD = ("batched mixed workload: {jobs} substrates of 10-500 beaded axons (40 spheres at 1 um, radii "
-                  "U[0.5,1.5], z-periodic, packed at area fraction 0.35), walkers log-uniform 1e4-1e6 (x{scale}), "
-                  "2000-8000 steps at dt=5 us (PGSE delta=te/3, Delta=2te/3), 6-60 directions, b={{0,1,2,3}} "
-                  "ms/um^2, seed 4")
+def _tuning_from_args(args, base):
+    if args.cell:
+        base.cell = args.cell
+    if args.steps_per_launch:
+        base.steps_per_launch = args.steps_per_launch
+    if args.coarsen:
+        base.coarsen = args.coarsen
+    if args.by_label is not None:
+        base.by_label = bool(args.by_label)
+    if args.near_margin is not None:
+        base.near_margin = args.near_margin if args.near_margin > 0 else None
+    return base
+
+
+def plain_leg(specs, positions, sig_batched, every: int):
+    """The plain per-substrate path on every `every`-th job, one job after
+    another (1 um cells): (walker-steps/s, jobs timed, walker-steps timed,
+    largest |S_plain - S_batched|)."""
+    import torch
+    from nozomi_b200.batch import SubstrateCache
+    from nozomi_b200.plain import run_plain
+    from nozomi_b200.simulate import Tuning
+    stream = torch.cuda.current_stream()
+    sel = list(range(0, len(specs), max(1, every)))
+    ms, ws, err = 0.0, 0, 0.0
+    tuning, cache = Tuning(), SubstrateCache()
+    for i in sel:
+        sp = specs[i]
+        dsub = cache.get(sp.key, sp.substrate, sp.D, sp.T2, tuning)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = run_plain(dsub, sp, positions[i][0])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        ws += sp.N * sp.nsteps
+        o = out.cpu().numpy()
+        err = max(err, float(np.abs((o[0] + 1j * o[1]) / sp.N - sig_batched[i]).max()))
+    return ws / (ms * 1e-3), len(sel), ws, err
+
+
+def serving_leg(pairs, tuning, threads, max_requests=None):
+    """Poisson request streams (configs of the mixed workload's distribution,
+    substrates reused with probability 0.7) through the continuous-batching
+    server, one stream per (rate, window).  Returns per-rate statistics,
+    substrate cache hits/misses and the host seconds spent generating the
+    streams' substrates."""
+    import torch
+    from nozomi_b200.batch import SubstrateCache
+    from nozomi_b200.serve import Server, latency_stats
+    from nozomi_b200.workloads import request_stream
+    cache = SubstrateCache()
+    per_rate, done_all = [], []
+    gen_s = 0.0
+    for rate, window in pairs:
+        t0 = time.perf_counter()
+        reqs = request_stream(rate, window, seed=5, max_requests=max_requests)
+        gen_s += time.perf_counter() - t0
+        srv = Server(tuning=tuning, threads=threads, cache=cache)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        done = srv.serve(reqs)
+        wall = time.perf_counter() - t0
+        st = latency_stats(done)
+        st.update({"rate_req_s": rate, "arrival_window_s": window, "requests": len(reqs),
+                   "walker_steps": srv.walker_steps, "walker_steps_per_s": srv.walker_steps / wall, "wall_s": wall,
+                   "rounds": srv.rounds, "failed": sum(t.error is not None for t in done)})
+        per_rate.append(st)
+        done_all += done
+    return per_rate, {"hits": cache.hits, "misses": cache.misses}, gen_s, done_all
 
 
 def run_batched(args):
     import torch
-    from nozomi_b200 import engine
-    from nozomi_b200.batch import BatchRun, SubstrateCache
-    from nozomi_b200.plain import run_plain
+    import torch.distributed as dist
+    from nozomi_b200 import engine, _lib as L
+    from nozomi_b200.batch import BatchRun, SubstrateCache, simulate_batch
+    from nozomi_b200.shard import init_process_group, shard_jobs
     from nozomi_b200.simulate import Tuning
     from nozomi_b200.workloads import mixed_specs
-    import torch.distributed as dist
-    from nozomi_b200.shard import init_process_group, shard_jobs
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
     if world > 1:
         init_process_group("nccl", timeout_s=180)
     engine.require_cuda()
+    t0 = time.perf_counter()
     all_specs = mixed_specs(seed=4, n_jobs=args.jobs, walker_scale=args.walker_scale)
+    gen_s = time.perf_counter() - t0
     # over several GPUs the jobs shard whole, longest first onto the least
-    # loaded rank; no data crosses ranks
+    # loaded rank; no data crosses ranks (strong scaling of a fixed batch)
     mine = shard_jobs([sp.walker_steps for sp in all_specs], world)[rank] if world > 1 else range(len(all_specs))
     specs = [all_specs[i] for i in mine]
-    tuning = Tuning()
-    if args.steps_per_launch:
-        tuning.steps_per_launch = args.steps_per_launch
-    if args.near_margin is not None:
-        tuning.near_margin = args.near_margin if args.near_margin > 0 else None
+    tuning = _tuning_from_args(args, Tuning())
     tune_report = None
     threads = args.threads
     if args.autotune:
         from nozomi_b200.autotune import autotune
         tuning, threads, tune_report = autotune(specs)
     cache = SubstrateCache()
-    run = BatchRun(specs, tuning=tuning, threads=threads, cache=cache)
     stream = torch.cuda.current_stream()
-    run.step()
-    for _ in range(max(0, args.warmup - 1)):
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run = BatchRun(specs, tuning=tuning, threads=threads, cache=cache)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    positions = run.seed_positions()
+    run.positions = positions
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    lib = L.load()
+    fp32_peak_tflops = fp32_peak(lib, L, stream, sms)
+    flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(1, args.warmup)):
         run.step()
+        flush.zero_()
+    barrier()
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph):
         run.step()
-    torch.cuda.synchronize()
-    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    graph.replay()
+    barrier()
+    clocks = Clocks(local)
     clocks.start()
     ms = 0.0
     for _ in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (outside the step's events)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -640,112 +824,166 @@ def run_batched(args):
         e1.record(stream)
         torch.cuda.synchronize()
         ms += e0.elapsed_time(e1)
+    barrier()
     clk = clocks.stop()
     del graph
+    sig_batched = run.signals()
+
+    # the same step launched eagerly with CUDA events around every batched
+    # walk launch: the dominant kernel's average launch and its share
+    ev = []
+    flush.zero_()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run.prepare().run(events=ev)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    eager_ms = e0.elapsed_time(e1)
+    walk_ms = sum(a.elapsed_time(b) for a, b in ev)
+    chunk_ws = [c["walker_steps"] for c in run.chunks]
+
+    # end to end through the public call: positions from pinned host memory,
+    # the batch planned, walked and reduced, the signals copied back
+    host_pos = [(x.cpu().pin_memory(), lab.cpu().pin_memory()) for x, lab in positions]
+    e2e_ms, io = 0.0, {}
+    for i in range(args.e2e_steps + 1):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sig_e2e = simulate_batch(specs, positions=host_pos, tuning=tuning, threads=threads, cache=cache, stats=io)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:  # the first pass warms the path
+            e2e_ms += e0.elapsed_time(e1)
+    e2e_diff = max(float(np.abs(a - b).max()) for a, b in zip(sig_e2e, sig_batched))
+
+    t_local = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
     if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t[0])
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(t_local[0]), float(t_local[1])
     ws = sum(sp.walker_steps for sp in all_specs)
     value = ws * args.steps / (ms * 1e-3)
-    sig_batched = run.signals()
-    if world > 1:  # the plain comparison is a one-GPU measurement
-        dist.barrier()
-        dist.destroy_process_group()
+    e2e_value = ws * args.e2e_steps / (e2e_ms * 1e-3) if args.e2e_steps else None
+    kernel_ws_s = sum(chunk_ws) / (walk_ms * 1e-3)
+    wl = BATCH_WORKLOAD.format(jobs=len(all_specs), scale=args.walker_scale)
+    config = {"workload": wl, "jobs": len(all_specs), "walker_steps_per_step": ws,
+              "walkers": sum(sp.N for sp in all_specs), "threads": threads,
+              "steps_per_launch": tuning.steps_per_launch, "near_margin_um": tuning.near_margin,
+              "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label,
+              "persistent_grid": run.grid, "chunks": len(run.chunks),
+              "l2": "256 MiB flush between timed steps (the inputs, 64 substrates' cell lists and walker "
+                    "state, are also larger than L2)",
+              "parallelism": (f"jobs sharded whole over {world} GPUs, longest first" if world > 1 else "one GPU")}
+    e2e = None if e2e_value is None else {
+        "value": e2e_value, "unit": "walker-steps/s", "h2d_bytes_per_step": int(io.get("h2d_bytes", 0)),
+        "d2h_bytes_per_step": int(io.get("d2h_bytes", 0)),
+        "call": "nozomi_b200.batch.simulate_batch(specs, positions=pinned host arrays): protocol tables, job, "
+                "item and re-binning tables built and uploaded, walkers packed, every chunk re-binned and walked "
+                "(eager launches), signals reduced and copied back; cell lists from a warm substrate cache",
+        "max_signal_diff_vs_graph": e2e_diff}
+    if world > 1:
         if rank == 0:
             print(json.dumps({"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
                               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                               "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
-                              "data": "synthetic (seeded substrates, protocols and walkers)",
-                              "config": {"workload": BATCH_WORKLOAD.format(jobs=len(all_specs),
-                                                                           scale=args.walker_scale),
-                                         "jobs": len(all_specs), "walker_steps_per_step": ws,
-                                         "parallelism": f"jobs sharded whole over {world} GPUs"},
-                              "clocks": clk}), flush=True)
+                              "data": "synthetic (seeded substrates, protocols and walkers)", "config": config,
+                              "e2e": e2e, "gpu_launches": run.launches() * args.steps, "clocks": clk}), flush=True)
+        dist.barrier()
+        dist.destroy_process_group()
         return 0
-    # the plain per-substrate path, one job after another, launched from the
-    # host, on cell lists of the default shape (1 um cells; not the batch's
-    # tuned shape, which the plain kernel does not benefit from)
-    sel = list(range(0, len(specs), args.plain_every))
-    plain_ms, plain_ws, err = 0.0, 0, 0.0
-    plain_tuning, plain_cache = Tuning(), SubstrateCache()
-    for i in sel:
-        sp = specs[i]
-        dsub = plain_cache.get(sp.key, sp.substrate, sp.D, sp.T2, plain_tuning)
-        x = run.positions[i][0]
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        out = run_plain(dsub, sp, x)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        plain_ms += e0.elapsed_time(e1)
-        plain_ws += sp.N * sp.nsteps
-        o = out.cpu().numpy()
-        err = max(err, float(np.abs((o[0] + 1j * o[1]) / sp.N - sig_batched[i]).max()))
-    plain_value = plain_ws / (plain_ms * 1e-3)
-    line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded substrates, protocols and walkers)",
-            "config": {"workload": BATCH_WORKLOAD.format(jobs=len(specs), scale=args.walker_scale),
-                       "jobs": len(specs), "walker_steps_per_step": ws, "threads": threads,
-                       "steps_per_launch": tuning.steps_per_launch, "near_margin_um": tuning.near_margin,
-                       "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen,
-                       "persistent_grid": run.grid, "chunks": len(run.chunks)},
+
+    plain = None
+    if not args.no_plain:
+        pv, pjobs, pws, perr = plain_leg(specs, positions, sig_batched, args.plain_every)
+        plain = {"value": pv, "unit": "walker-steps/s", "jobs_timed": pjobs, "every": args.plain_every,
+                 "walker_steps_timed": pws, "cell_um": 1.0, "max_signal_diff_vs_batched": perr,
+                 "launch": "one plain-kernel launch per waveform sample from the host, per-direction phase in "
+                           "HBM, jobs one after another (every k-th job of the batch)"}
+    serving = None
+    if not args.no_serving:
+        pairs = [tuple(float(v) for v in p.split(":")) for p in args.serve.split(",") if p]
+        stune = Tuning(cell=args.serve_cell or tuning.cell, coarsen=args.serve_coarsen or tuning.coarsen,
+                       near_margin=tuning.near_margin, by_label=tuning.by_label)
+        per_rate, sc, sgen, _ = serving_leg(pairs, stune, threads, args.max_requests)
+        serving = {"per_rate": per_rate, "substrate_cache": sc, "substrate_generation_s": sgen,
+                   "cell_um": stune.cell, "rebin_coarsen": stune.coarsen,
+                   "rounds": "time-bounded (about 50 ms at the measured throughput, 100-4000 steps)",
+                   "admission": "side stream, overlapping the running round"}
+        if plain:
+            for r in per_rate:
+                r["speedup_vs_plain"] = r["walker_steps_per_s"] / plain["value"]
+    cpu, wk_all = None, None
+    if not args.no_cpu_baseline:
+        cases, what = reference_cases("batched")
+        try:
+            v, cores, sample, _ = reference_cpu_sample(cases, args.cpu_seconds / 2)
+            cpu = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "reference",
+                   "sample": f"{what}: {sample}; {REF_CPU_KIND}"}
+        except (FileNotFoundError, ValueError) as e:
+            v, cores, sample = port_sample(cases, args.cpu_seconds / 2)
+            cpu = {"value": v, "unit": "walker-steps/s", "cores": cores, "kind": "port",
+                   "sample": f"{what}: {sample}; oracle/walk_oracle.c, OpenMP over walkers",
+                   "reference_unavailable": str(e)}
+        # algorithmic work per walker-step from the oracle's count mode on the
+        # sampled jobs (the lists of the batch's cell size)
+        works = [cpu_sample(sub, gw, dirs, tuning.cell, 0.5, work=True)[3] for _, sub, gw, dirs in cases]
+        wk_all = {k: float(np.mean([w[k] for w in works])) for k in works[0]}
+    ndir_mean = sum(sp.walker_steps * np.asarray(sp.dirs).shape[1] for sp in specs) / ws
+    F_alg = None if wk_all is None else 10 * wk_all["spheres_in_reach"] + 36 * wk_all["solves_in_reach"] + 6 * ndir_mean
+    launch_ms = walk_ms / max(len(ev), 1)
+    ws_launch = sum(chunk_ws) / max(len(chunk_ws), 1)
+    state_bytes = 128 * sum(c["sort_walkers"] for c in run.chunks) / max(len(run.chunks), 1)
+    roof_issue, roof_fp32, roof_hbm = rooflines("batched", kernel_ws_s, ws_launch, launch_ms, state_bytes, clk, sms,
+                                                fp32_peak_tflops, F_alg, wk_all)
+    line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded substrates, protocols and walkers)", "config": config,
+            "speedup_vs_plain": None if plain is None else value / plain["value"],
+            "plain": plain, "serving": serving, "e2e": e2e,
+            "gpu_launches": run.launches() * args.steps,
+            "kernel": {"name": "walk_fused_kernel (batched form, nz_walk_batch)", "launches": len(ev),
+                       "avg_launch_ms": launch_ms, "walker_steps_per_launch": ws_launch,
+                       "kernel_walker_steps_per_s": kernel_ws_s, "share_of_step": walk_ms / eager_ms,
+                       "eager_step_ms": eager_ms, "walker_steps_per_chunk": chunk_ws,
+                       "timing": "value from CUDA-graph replays of the step; kernel figures from one eager "
+                                 "step with events around each batched launch"},
+            "setup": {"substrate_generation_s": gen_s, "device_substrates_s": build_s,
+                      "timing": "host generation of the 64 seeded substrates and their one-time device cell "
+                                "lists (wall clock); not part of value"},
             "autotune": None if tune_report is None else {
                 "cached": tune_report["cached"], "choice": {"threads": threads, **dataclasses.asdict(tuning)},
                 "trials": len(tune_report.get("trials", [])),
                 "trial_walker_steps_per_s": tune_report.get("trial_walker_steps_per_s")},
-            "gpu_launches": run.launches() * args.steps,
-            "plain": {"value": plain_value, "unit": "walker-steps/s", "jobs_timed": len(sel),
-                      "walker_steps_timed": plain_ws, "cell_um": plain_tuning.cell,
-                      "launch": "one plain-kernel launch per step from the host, "
-                      "per-direction phase in HBM, substrates one after another"},
-            "speedup_vs_plain": value / plain_value,
-            "max_signal_diff_batched_vs_plain": err, "clocks": clk}
+            "roofline": roof_issue, "roofline_fp32": roof_fp32, "roofline_hbm": roof_hbm,
+            "cpu_baseline": cpu, "clocks": clk}
     print(json.dumps(line), flush=True)
     return 0
 
 
 def run_serving(args):
+    """The request streams alone (--serve rate:window pairs), with the plain
+    kernel timed on a sample of the served requests."""
     import torch
     if int(os.environ.get("RANK", "0")) != 0:  # a one-GPU request loop
         return 0
     from nozomi_b200 import engine
     from nozomi_b200.batch import SubstrateCache
     from nozomi_b200.plain import run_plain
-    from nozomi_b200.serve import Server, latency_stats
     from nozomi_b200.simulate import Tuning
-    from nozomi_b200.workloads import request_stream
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     engine.require_cuda()
-    # the cell lists and re-binning of the autotuner's choice for this
-    # substrate distribution (1.5 um cells, 12 um bins); a round is 500 steps
-    tuning = Tuning(cell=args.serve_cell, coarsen=args.serve_coarsen, steps_per_launch=500)
-    if args.steps_per_launch:
-        tuning.steps_per_launch = args.steps_per_launch
-    cache = SubstrateCache()
-    per_rate = []
-    all_done = []
+    tuning = _tuning_from_args(args, Tuning())
+    if args.serve_cell:
+        tuning.cell = args.serve_cell
+    if args.serve_coarsen:
+        tuning.coarsen = args.serve_coarsen
+    pairs = [tuple(float(v) for v in p.split(":")) for p in args.serve.split(",") if p]
     clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
-    for rate in [float(r) for r in args.rates.split(",")]:
-        reqs = request_stream(rate, min(args.serve_seconds, args.max_requests / rate), seed=5,
-                              max_requests=args.max_requests)
-        # warm the substrate cache's first entries so every rate starts from the same state
-        srv = Server(tuning=tuning, threads=args.threads, cache=cache)
-        t0 = time.perf_counter()
-        done = srv.serve(reqs)
-        wall = time.perf_counter() - t0
-        st = latency_stats(done)
-        st.update({"rate_req_s": rate, "requests": len(reqs), "walker_steps": srv.walker_steps,
-                   "walker_steps_per_s": srv.walker_steps / wall, "wall_s": wall, "rounds": srv.rounds,
-                   "failed": sum(t.error is not None for t in done)})
-        per_rate.append(st)
-        all_done += done
+    per_rate, sc, sgen, all_done = serving_leg(pairs, tuning, args.threads, args.max_requests)
     clk = clocks.stop()
-    # the plain per-substrate kernel on a sample of the same requests, one
-    # after another, on cell lists of the default shape (1 um cells)
     sample = all_done[:: max(1, len(all_done) // 8)][:8]
     stream = torch.cuda.current_stream()
     pms, pws = 0.0, 0
@@ -763,23 +1001,19 @@ def run_serving(args):
         pms += e0.elapsed_time(e1)
         pws += sp.N * sp.nsteps
     plain_value = pws / (pms * 1e-3)
-    total_ws = sum(r["walker_steps"] for r in per_rate)
-    total_wall = sum(r["wall_s"] for r in per_rate)
-    value = total_ws / total_wall
+    value = sum(r["walker_steps"] for r in per_rate) / sum(r["wall_s"] for r in per_rate)
     line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
             "steps": len(per_rate), "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded Poisson request streams)",
             "config": {"workload": "serving: Poisson arrivals per rate, substrates of 10-500 beaded axons reused "
                                    "with probability 0.7, 1e4-5e5 walkers, 2000-8000 steps at 5 us, 6-60 directions, "
-                                   "b<=3 ms/um^2, seed 5", "rates": args.rates,
-                       "arrival_window_s": args.serve_seconds, "max_requests_per_rate": args.max_requests,
-                       "steps_per_launch": tuning.steps_per_launch, "threads": args.threads,
+                                   "b<=3 ms/um^2, seed 5", "rates_and_windows": args.serve,
+                       "max_requests_per_rate": args.max_requests, "threads": args.threads,
                        "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen},
-            "per_rate": per_rate,
+            "per_rate": per_rate, "substrate_generation_s": sgen,
             "plain": {"value": plain_value, "unit": "walker-steps/s", "requests_timed": len(sample),
                       "launch": "one plain-kernel launch per step, requests one after another"},
-            "speedup_vs_plain": value / plain_value, "substrate_cache": {"hits": cache.hits, "misses": cache.misses},
-            "clocks": clk}
+            "speedup_vs_plain": value / plain_value, "substrate_cache": sc, "clocks": clk}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -801,7 +1035,7 @@ def run_reference_gpu(args):
         return 0
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     engine.require_cuda()
-    sub, pg, dirs, bvals = workload()
+    sub, pg, dirs, bvals = workload_packed()
     ref = RefGpuWalk("packed_1e6")
     N = ref.N
     dsub = device_substrate(sub, D=2.0, T2=100.0, cell=1.0)
@@ -918,19 +1152,19 @@ def run_narrow(args):
     return 0
 
 
-def main():
-    args = parse()
+def main(argv=None):
+    args = parse(argv)
     if args.impl == "reference":
         return run_reference(args)
     if args.impl == "reference_gpu":
         return run_reference_gpu(args)
-    if args.workload == "batched":
-        return run_batched(args)
+    if args.workload == "packed":
+        return run_packed(args)
     if args.workload == "serving":
         return run_serving(args)
     if args.workload == "narrow":
         return run_narrow(args)
-    return run_ours(args)
+    return run_batched(args)
 
 
 if __name__ == "__main__":

@@ -260,6 +260,34 @@ int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarsen, nz_state
 int nz_state_sort_keyed(const nz_state* in, const nz_grid* grid, int coarsen, int nlabels, nz_state* out,
                         void* scratch, size_t scratch_bytes, void* stream);
 
+/* ---- the re-binning of many jobs at once (the batched walk's step between
+ * chunks): one bin count, one scan and one scatter for every job of a chunk,
+ * instead of a sort per job.  No reference counterpart (the reference runs
+ * one substrate at a time and re-bins nothing).  Job j's walkers take keys
+ * [key_offset, key_offset + nz_sort_job_keys(...)) of one key space, its
+ * local key being nz_state_sort_keyed's; the walkers are counted and
+ * scattered in one pass over all jobs' walkers, and job j's land in its own
+ * out state.  walker_offset = the sum of N of the jobs before it. ---- */
+typedef struct nz_sort_job {
+    nz_state in;           /* the job's walkers (read) */
+    nz_state out;          /* receives them re-binned: same N, no array shared with in */
+    nz_grid grid;          /* the job's cell grid */
+    int coarsen;           /* bins = cells coarsened by this factor per axis */
+    int nlabels;           /* > 0: key (label, bin) as nz_state_sort_keyed; 0: bin */
+    int walker_offset;
+    int key_offset;
+} nz_sort_job;
+
+/* Keys of one job: bins, times nlabels when nlabels > 0; -1 for a bad grid. */
+long long nz_sort_job_keys(const nz_grid* grid, int coarsen, int nlabels);
+size_t nz_batch_sort_scratch_bytes(int total_walkers, int total_keys);
+/* jobs: a device array of n_jobs descriptors, in walker_offset order, whose
+ * walker_offset / key_offset are the running sums above (the caller
+ * guarantees them; the device array is not read back for checking);
+ * total_walkers / total_keys: the sums over all jobs. */
+int nz_batch_sort(const nz_sort_job* jobs, int n_jobs, int total_walkers, int total_keys, void* scratch,
+                  size_t scratch_bytes, void* stream);
+
 /* Re-binning for callers that cannot allocate device memory (no counterpart in
  * the reference, which re-bins nothing).  Same result as nz_state_sort, but the
  * scratch is a fixed 16 MiB device array inside the library (one per GPU that

@@ -58,6 +58,11 @@ class Item(ctypes.Structure):
     _fields_ = [("job", _i), ("first", _i), ("count", _i)]
 
 
+class SortJob(ctypes.Structure):
+    _fields_ = [("inp", State), ("out", State), ("grid", Grid), ("coarsen", _i), ("nlabels", _i),
+                ("walker_offset", _i), ("key_offset", _i)]
+
+
 # name -> (restype, argtypes); every symbol of include/nozomi_b200.h
 SIGNATURES = {
     "nz_version": (_i, []),
@@ -83,6 +88,9 @@ SIGNATURES = {
     "nz_sort_scratch_bytes": (ctypes.c_size_t, [_i, _i]),
     "nz_state_sort": (_i, [_P, _P, _i, _P, _P, ctypes.c_size_t, _P]),
     "nz_state_sort_keyed": (_i, [_P, _P, _i, _i, _P, _P, ctypes.c_size_t, _P]),
+    "nz_sort_job_keys": (ctypes.c_longlong, [_P, _i, _i]),
+    "nz_batch_sort_scratch_bytes": (ctypes.c_size_t, [_i, _i]),
+    "nz_batch_sort": (_i, [_P, _i, _i, _i, _P, ctypes.c_size_t, _P]),
     "nz_state_sort_static_capacity": (ctypes.c_size_t, []),
     "nz_state_sort_static": (_i, [_P, _P, _i, _P, _P]),
     "nz_signal_phi": (_i, [_P, _P, _i, _P, _i, _P, _P]),

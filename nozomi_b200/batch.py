@@ -8,7 +8,9 @@ sample (diffsim3d.py:246-261).  Here every job of a batch advances together:
     of ``steps_per_launch`` steps, one launch of ``nz_walk_batch`` runs every
     item of every job that still has steps, CTAs taking items from a queue
     (longest first) until it is empty;
-  * between chunks every active job's walkers are re-binned by (label, cell);
+  * before every chunk the walkers of all its jobs are re-binned by (label,
+    cell) in one pass (``nz_batch_sort``: one bin count, one scan, one
+    scatter over every job's walkers);
   * after the last chunk each job's signal is reduced on the device;
   * draws are keyed by (job seed, walker id, step), so a job's result does not
     depend on what it was batched with (test_batch.py checks alone vs mixed).
@@ -108,16 +110,47 @@ def _job_table(jobs, states) -> torch.Tensor:
     return torch.from_numpy(raw).cuda()
 
 
+def _sort_table(pairs, coarsen, by_label):
+    """nz_sort_job[] of one chunk's re-binning (bytes on the device), with
+    the total walker and key counts.  pairs: (job dict, source state,
+    destination state) of every active job."""
+    lib = L.load()
+    arr = (L.SortJob * max(1, len(pairs)))()
+    tw = tk = 0
+    for i, (j, src, dst) in enumerate(pairs):
+        g = j["sub"].grid
+        nl = j["sub"].nstructures + 1 if by_label else 0
+        keys = int(lib.nz_sort_job_keys(L.byref(g), int(coarsen), nl))
+        if keys <= 0:
+            raise L.NozomiError(f"re-binning: bad grid or coarsening for job {i}")
+        arr[i].inp, arr[i].out = src.struct(), dst.struct()
+        arr[i].grid = g
+        arr[i].coarsen, arr[i].nlabels = int(coarsen), nl
+        arr[i].walker_offset, arr[i].key_offset = tw, tk
+        tw += src.N
+        tk += keys
+    if tw >= 2 ** 31 or tk >= 2 ** 31:
+        raise L.NozomiError(f"re-binning: {tw} walkers / {tk} keys in one chunk exceed the int range")
+    raw = np.frombuffer(bytes(arr), dtype=np.uint8).copy()
+    return torch.from_numpy(raw).cuda(), len(pairs), tw, tk
+
+
 def _items(jobs, active, threads, s0, k) -> torch.Tensor:
-    """Items of the active jobs, longest remaining work first."""
-    rows = []
+    """Items (job, first walker, count) of the active jobs, longest remaining
+    work first (ties in job, then walker order)."""
+    parts, work = [], []
     for j in active:
+        N = int(jobs[j]["N"])
         steps = min(k, jobs[j]["nsteps"] - s0)
-        for first in range(0, jobs[j]["N"], threads):
-            rows.append((steps * min(threads, jobs[j]["N"] - first), j, first, min(threads, jobs[j]["N"] - first)))
-    rows.sort(key=lambda r: -r[0])
-    it = np.array([[r[1], r[2], r[3]] for r in rows], np.int32).reshape(-1, 3)
-    return torch.from_numpy(it).cuda()
+        first = np.arange(0, N, threads, dtype=np.int64)
+        count = np.minimum(threads, N - first)
+        parts.append(np.stack([np.full(first.size, j), first, count], axis=1))
+        work.append(steps * count)
+    if not parts:
+        return torch.zeros((0, 3), dtype=torch.int32, device="cuda")
+    it, w = np.concatenate(parts), np.concatenate(work)
+    it = it[np.argsort(-w, kind="stable")].astype(np.int32)
+    return torch.from_numpy(np.ascontiguousarray(it)).cuda()
 
 
 class BatchRun:
@@ -145,6 +178,10 @@ class BatchRun:
                 "seed": int(sp.seed),
             })
         self.positions = positions
+        # bytes copied host -> device per step: protocol tables, directions
+        # and amplitudes above, plus positions given as host arrays and the
+        # chunk tables (added by prepare)
+        self.h2d_bytes = sum(j["G"].numel() * 8 + j["dirs"].numel() * 4 + j["amps"].numel() * 4 for j in self.jobs)
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         occ = ctypes.c_int(0)
         L.check(L.load().nz_batch_occupancy(L.MODE_PHI, self.threads, ctypes.byref(occ)), "nz_batch_occupancy")
@@ -161,17 +198,32 @@ class BatchRun:
 
     def prepare(self, positions=None):
         """Pack walker state (both ping-pong buffers), plan the chunks and
-        upload their job tables and item lists."""
+        upload their job tables, re-binning tables and item lists.
+
+        positions: per job (positions [3, N], labels [N] or None) as device
+        tensors, or as host arrays (numpy or CPU tensors, pinned for an
+        asynchronous copy), which are copied to the device here; None: the
+        positions given at construction, else walkers seeded on the device."""
         if positions is None:
             positions = self.positions if self.positions is not None else self.seed_positions()
-        self.positions = positions
-        for j, (x, lab) in zip(self.jobs, positions):
+        dev = torch.device("cuda", torch.cuda.current_device())
+        placed = []
+        for x, lab in positions:
+            if not (isinstance(x, torch.Tensor) and x.is_cuda):
+                x = torch.as_tensor(x, dtype=torch.float32)
+                self.h2d_bytes += x.numel() * 4
+                x = x.to(dev, non_blocking=True)
+            if lab is not None and not (isinstance(lab, torch.Tensor) and lab.is_cuda):
+                lab = torch.as_tensor(lab, dtype=torch.int32)
+                self.h2d_bytes += lab.numel() * 4
+                lab = lab.to(dev, non_blocking=True)
+            placed.append((x, lab))
+        self.positions = placed
+        for j, (x, lab) in zip(self.jobs, placed):
             if "buf" not in j:  # allocated once: the chunk tables point at these buffers
                 j["buf"] = [engine.FusedState(j["N"]), engine.FusedState(j["N"])]
-                j["scratch"] = None
             wk = engine.Walkers(x, x.clone(), phi=torch.zeros((6, j["N"]), device=x.device), label=lab)
             j["buf"][0].pack(wk)
-            j["cur"] = 0
         if not self._planned:
             self._plan()
         return self
@@ -181,40 +233,54 @@ class BatchRun:
         nmax = max(j["nsteps"] for j in self.jobs)
         self.chunks = []
         cur = [0] * len(self.jobs)
+        need = 0
         for s0 in range(0, nmax, k):
             active = [i for i, j in enumerate(self.jobs) if j["nsteps"] > s0]
+            pairs = [(self.jobs[i], self.jobs[i]["buf"][cur[i]], self.jobs[i]["buf"][cur[i] ^ 1]) for i in active]
             for i in active:
                 cur[i] ^= 1
             states = [self.jobs[i]["buf"][cur[i]] for i in range(len(self.jobs))]
+            sort, n_sort, tw, tk = _sort_table(pairs, self.tuning.coarsen, self.tuning.by_label)
+            need = max(need, int(L.load().nz_batch_sort_scratch_bytes(tw, tk)))
+            items = _items(self.jobs, active, self.threads, s0, k)
+            ws = sum(min(k, self.jobs[i]["nsteps"] - s0) * self.jobs[i]["N"] for i in active)
             self.chunks.append({"s0": s0, "s1": s0 + k, "active": active, "table": _job_table(self.jobs, states),
-                                "items": _items(self.jobs, active, self.threads, s0, k)})
+                                "items": items, "sort": sort, "n_sort": n_sort, "sort_walkers": tw,
+                                "sort_keys": tk, "walker_steps": ws})
+            self.h2d_bytes += sort.numel() + items.numel() * 4 + self.chunks[-1]["table"].numel()
         self.final_cur = cur
+        self.sort_scratch = torch.empty(max(need, 1), dtype=torch.uint8, device="cuda")
         self.queue = torch.zeros(len(self.chunks), dtype=torch.int32, device="cuda")
         self.out = [torch.zeros((2, j["dirs"].shape[1], j["amps"].numel()), dtype=torch.float64, device="cuda")
                     for j in self.jobs]
         self._planned = True
 
     # -- the run -------------------------------------------------------------------
-    def run(self):
+    def run(self, events: list | None = None):
+        """Every chunk: one re-binning of all its jobs, one batched walk; then
+        each job's signal.  events: if a list, (start, end) CUDA events of each
+        batched walk launch are appended to it."""
         lib = L.load()
-        nl_on = self.tuning.by_label
-        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        cs = torch.cuda.current_stream()
+        stream = ctypes.c_void_p(cs.cuda_stream)
         self.queue.zero_()
-        for c in self.chunks:
-            for i in c["active"]:
-                j = self.jobs[i]
-                src, dst = j["buf"][j["cur"]], j["buf"][j["cur"] ^ 1]
-                j["scratch"] = src.sort_into(dst, j["sub"].grid, self.tuning.coarsen, j["scratch"],
-                                             nlabels=j["sub"].nstructures + 1 if nl_on else 0)
-                j["cur"] ^= 1
-            qi = self.chunks.index(c)
+        for qi, c in enumerate(self.chunks):
+            L.check(lib.nz_batch_sort(ctypes.c_void_p(c["sort"].data_ptr()), c["n_sort"], c["sort_walkers"],
+                                      c["sort_keys"], ctypes.c_void_p(self.sort_scratch.data_ptr()),
+                                      self.sort_scratch.numel(), stream), "nz_batch_sort")
+            if events is not None:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(cs)
             L.check(lib.nz_walk_batch(ctypes.c_void_p(c["table"].data_ptr()), len(self.jobs),
                                       ctypes.c_void_p(c["items"].data_ptr()), int(c["items"].shape[0]), L.MODE_PHI,
                                       c["s0"], c["s1"], ctypes.c_void_p(self.queue.data_ptr() + 4 * qi), self.grid,
                                       self.threads, stream), "nz_walk_batch")
-        for j, out in zip(self.jobs, self.out):
+            if events is not None:
+                e1.record(cs)
+                events.append((e0, e1))
+        for i, (j, out) in enumerate(zip(self.jobs, self.out)):
             out.zero_()
-            j["buf"][j["cur"]].signal(j["dirs"], j["amps"], out)
+            j["buf"][self.final_cur[i]].signal(j["dirs"], j["amps"], out)
         return self
 
     def step(self):
@@ -223,27 +289,47 @@ class BatchRun:
 
     def launches(self) -> int:
         """Library kernels of one step (prepare + run): a pack per job; per
-        chunk each active job's re-binning (FusedState.sort_kernels) and one
-        batched walk; a signal per job."""
-        nl_on = self.tuning.by_label
+        chunk the re-binning of all its jobs (bin count, the key scan: one
+        kernel, or three above SCAN_SINGLE_KEYS keys, scatter) and one batched
+        walk; a signal per job."""
         n = sum(1 for j in self.jobs if j["N"]) * 2  # pack and signal
         for c in self.chunks:
-            for i in c["active"]:
-                j = self.jobs[i]
-                n += j["buf"][0].sort_kernels(j["sub"].grid, self.tuning.coarsen,
-                                              j["sub"].nstructures + 1 if nl_on else 0)
+            if c["sort_walkers"]:
+                n += 2 + (1 if c["sort_keys"] <= L.SCAN_SINGLE_KEYS else 3)
             n += 1 if c["items"].shape[0] else 0
         return n
 
     def signals(self) -> list:
+        """Per job S[d][b] (complex, normalised by N), copied to the host."""
         res = []
         for j, out in zip(self.jobs, self.out):
             s = out.cpu().numpy()
             res.append((s[0] + 1j * s[1]) / j["N"])
         return res
 
+    def d2h_bytes(self) -> int:
+        return sum(out.numel() * out.element_size() for out in self.out)
+
     def walker_steps(self) -> int:
         return sum(j["N"] * j["nsteps"] for j in self.jobs)
 
     def final_state(self, i: int) -> engine.FusedState:
         return self.jobs[i]["buf"][self.final_cur[i]]
+
+
+def simulate_batch(specs: list, positions=None, tuning: Tuning | None = None, threads: int = 128,
+                   cache: SubstrateCache | None = None, stats: dict | None = None) -> list:
+    """Signals of many solves at once: S[d][b] (complex, per job) for every
+    JobSpec, walked together in persistent batched launches.
+
+    positions: per job (positions [3, N], labels [N] or None) on the host or
+    the device, or None to seed every job on the device.  cache: a
+    SubstrateCache to keep the cell lists of repeated substrates between
+    calls.  stats: if a dict, receives the bytes copied host -> device
+    ("h2d_bytes") and device -> host ("d2h_bytes") by this call."""
+    run = BatchRun(specs, tuning=tuning, threads=threads, cache=cache)
+    out = run.prepare(positions).run().signals()
+    if stats is not None:
+        stats["h2d_bytes"] = int(run.h2d_bytes)
+        stats["d2h_bytes"] = int(run.d2h_bytes())
+    return out

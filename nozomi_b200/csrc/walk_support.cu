@@ -98,6 +98,67 @@ __global__ void bin_scatter_kernel(nz_state in, int N, const int* __restrict__ b
 }
 
 // ---------------------------------------------------------------------------
+// Re-binning of many jobs in one pass: each thread finds its walker's job by a
+// binary search over the jobs' walker offsets, then keys it as bin_count_kernel
+// does, shifted into the job's key range.  The exclusive scan over the whole
+// key space gives each key's first slot in the concatenation of all jobs'
+// walkers; a job's walkers occupy [walker_offset, walker_offset + N) of it.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int job_of(const nz_sort_job* __restrict__ jobs, int n_jobs, int g) {
+  int lo = 0, hi = n_jobs - 1;  // the last job whose walker_offset <= g
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&jobs[mid].walker_offset) <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ BinGrid bin_grid_of(const nz_grid& grid, int coarsen, int nlabels) {
+  BinGrid b;
+  b.g = Grid{grid.Lx, grid.Ly, grid.Lz, grid.dLx, grid.dLy, grid.dLz, float(grid.nx), float(grid.ny), float(grid.nz)};
+  b.cx = b.cy = b.cz = coarsen;
+  b.bx = (grid.nx + coarsen - 1) / coarsen;
+  b.by = (grid.ny + coarsen - 1) / coarsen;
+  b.bz = (grid.nz + coarsen - 1) / coarsen;
+  b.nlabels = nlabels;
+  return b;
+}
+
+__global__ void batch_bin_count_kernel(const nz_sort_job* __restrict__ jobs, int n_jobs, int total,
+                                       int* __restrict__ bins, int* __restrict__ hist) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int j = job_of(jobs, n_jobs, g);
+  const nz_sort_job& J = jobs[j];
+  const BinGrid b = bin_grid_of(J.grid, J.coarsen, J.nlabels);
+  const float4 p = reinterpret_cast<const float4*>(J.in.pos)[g - J.walker_offset];
+  int k = bin_of(b, p.x, p.y, p.z);
+  if (b.nlabels > 0) {
+    int label = __float_as_int(p.w);
+    if (label < 0 || label >= b.nlabels) label = b.nlabels - 1;
+    k += label * (b.bx * b.by * b.bz);
+  }
+  k += J.key_offset;
+  bins[g] = k;
+  atomicAdd(hist + k, 1);
+}
+
+__global__ void batch_bin_scatter_kernel(const nz_sort_job* __restrict__ jobs, int n_jobs, int total,
+                                         const int* __restrict__ bins, int* __restrict__ cursor) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int j = job_of(jobs, n_jobs, g);
+  const nz_sort_job& J = jobs[j];
+  const int w = g - J.walker_offset;
+  const int slot = atomicAdd(cursor + bins[g], 1) - J.walker_offset;
+  reinterpret_cast<float4*>(J.out.pos)[slot] = reinterpret_cast<const float4*>(J.in.pos)[w];
+  reinterpret_cast<float4*>(J.out.org)[slot] = reinterpret_cast<const float4*>(J.in.org)[w];
+  reinterpret_cast<float4*>(J.out.phi)[slot] = reinterpret_cast<const float4*>(J.in.phi)[w];
+  reinterpret_cast<float4*>(J.out.comp)[slot] = reinterpret_cast<const float4*>(J.in.comp)[w];
+}
+
+// ---------------------------------------------------------------------------
 // Signal: S[d][b] += sum_w exp(i amp[b] u_d . Phi_w); FP32 per walker, FP64
 // block sums, one FP64 atomic per block and (d, b).
 // ---------------------------------------------------------------------------
@@ -298,6 +359,46 @@ extern "C" int nz_state_sort_keyed(const nz_state* in, const nz_grid* grid, int 
   if (rc) return rc;
   bin_scatter_kernel<<<(N + 255) / 256, 256, 0, st>>>(*in, N, bins, cursor, *out);
   return check_launch("bin_scatter_kernel");
+}
+
+extern "C" long long nz_sort_job_keys(const nz_grid* grid, int coarsen, int nlabels) {
+  if (!grid || grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0 || coarsen <= 0 || nlabels < 0) return -1;
+  return 1ll * ((grid->nx + coarsen - 1) / coarsen) * ((grid->ny + coarsen - 1) / coarsen) *
+         ((grid->nz + coarsen - 1) / coarsen) * (nlabels > 0 ? nlabels : 1);
+}
+
+extern "C" size_t nz_batch_sort_scratch_bytes(int total_walkers, int total_keys) {
+  return nz_sort_scratch_bytes(total_walkers, total_keys);
+}
+
+extern "C" int nz_batch_sort(const nz_sort_job* jobs, int n_jobs, int total_walkers, int total_keys, void* scratch,
+                             size_t scratch_bytes, void* stream) {
+  if (n_jobs < 0 || total_walkers < 0 || total_keys < 0 || (n_jobs > 0 && !jobs) ||
+      (total_walkers > 0 && (n_jobs == 0 || total_keys == 0)))
+    return set_error(NZ_ERR_ARG, "nz_batch_sort: bad arguments (jobs=%d walkers=%d keys=%d)", n_jobs, total_walkers,
+                     total_keys);
+  if (total_walkers == 0) return NZ_OK;
+  const size_t need = nz_sort_scratch_bytes(total_walkers, total_keys);
+  if (!scratch || scratch_bytes < need)
+    return set_error(NZ_ERR_CAPACITY, "nz_batch_sort: scratch %zu bytes < %zu", scratch_bytes, need);
+  char* p = static_cast<char*>(scratch);
+  const size_t nw = align256(size_t(total_walkers) * sizeof(int)), nk = align256(size_t(total_keys) * sizeof(int));
+  int* bins = reinterpret_cast<int*>(p);
+  int* hist = reinterpret_cast<int*>(p + nw);
+  int* cursor = reinterpret_cast<int*>(p + nw + nk);
+  int* tile_sums = reinterpret_cast<int*>(p + nw + 2 * nk);
+  int* tile_offsets = reinterpret_cast<int*>(p + nw + 2 * nk + align256(size_t(scan_tiles(total_keys)) * sizeof(int)));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(hist, 0, size_t(total_keys) * sizeof(int), st) != cudaSuccess)
+    return check_launch("nz_batch_sort memset");
+  const unsigned blocks = unsigned((total_walkers + 255) / 256);
+  batch_bin_count_kernel<<<blocks, 256, 0, st>>>(jobs, n_jobs, total_walkers, bins, hist);
+  int rc = check_launch("batch_bin_count_kernel");
+  if (rc) return rc;
+  rc = exclusive_scan(hist, cursor, total_keys, tile_sums, tile_offsets, st);
+  if (rc) return rc;
+  batch_bin_scatter_kernel<<<blocks, 256, 0, st>>>(jobs, n_jobs, total_walkers, bins, cursor);
+  return check_launch("batch_bin_scatter_kernel");
 }
 
 extern "C" int nz_state_sort(const nz_state* in, const nz_grid* grid, int coarsen, nz_state* out, void* scratch,

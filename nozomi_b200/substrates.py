@@ -200,6 +200,46 @@ def _pack_centres(req: np.ndarray, box, rng, max_iter: int):
     raise RuntimeError(f"packing did not converge (largest overlap {worst:.3g} um)")
 
 
+def _pack_centres_near(req: np.ndarray, box, rng, max_iter: int):
+    """_pack_centres with the overlaps of each relaxation step taken only over
+    pairs closer than the largest required distance (a periodic k-d tree's
+    pair query), O(n log n) per step instead of O(n^2): the same start, the
+    same update rule, rounding aside."""
+    from scipy.spatial import cKDTree
+    n = req.shape[0]
+    Lx, Ly = box
+    nx = max(1, int(np.ceil(np.sqrt(n * Lx / Ly))))
+    ny = max(1, int(np.ceil(n / nx)))
+    gx, gy = np.meshgrid((np.arange(nx) + 0.5) * Lx / nx - Lx / 2, (np.arange(ny) + 0.5) * Ly / ny - Ly / 2)
+    cells = rng.permutation(nx * ny)[:n]
+    P = np.stack([gx.ravel()[cells], gy.ravel()[cells]], axis=1)
+    P += rng.uniform(-0.25, 0.25, P.shape) * np.array([Lx / nx, Ly / ny])
+    b = np.array([Lx, Ly])
+    rc = float(req.max())
+    worst = np.inf
+    for it in range(max_iter):
+        Q = np.mod(P + b / 2, b)
+        Q[Q >= b] = 0.0
+        pairs = cKDTree(Q, boxsize=b).query_pairs(rc, output_type="ndarray")
+        if pairs.size == 0:
+            return P, it
+        i, j = pairs[:, 0], pairs[:, 1]
+        d = P[i] - P[j]
+        d -= b * np.round(d / b)
+        dist = np.sqrt((d ** 2).sum(-1))
+        ov = np.maximum(0.0, req[i, j] - dist)
+        worst = ov.max()
+        if worst < 1e-9:
+            return P, it
+        f = (ov / dist)[:, None] * d * 0.5
+        disp = np.zeros_like(P)
+        np.add.at(disp, i, f)
+        np.add.at(disp, j, -f)
+        P = P + disp
+        P = (P + b / 2) % b - b / 2
+    raise RuntimeError(f"packing did not converge (largest overlap {worst:.3g} um)")
+
+
 def _axons_with_images(P, R, z, L, image_margin):
     Lx, Ly, Lz = L
     dz = z[1] - z[0]
@@ -256,7 +296,7 @@ def axon_bundle(n_axons: int, seed: int, spheres_per_axon: int = 40, Lz: float =
     R = rng.uniform(r_range[0], r_range[1], (n_axons, spheres_per_axon))
     side = float(np.sqrt(np.pi * (R ** 2).mean(1).sum() / area_fraction))
     req = _required_distances(R, dz) + gap
-    P, it = _pack_centres(req, (side, side), rng, 20000)
+    P, it = _pack_centres_near(req, (side, side), rng, 20000)
     fibers = _axons_with_images(P, R, z, (side, side, Lz), image_margin)
     return Substrate(fibers, (side, side, Lz), {"kind": "axon_bundle", "n_axons": n_axons, "seed": seed,
                                                  "relax_iterations": it})

@@ -77,7 +77,7 @@ def calibration_substrate() -> Substrate:
 
 def bundle(n_axons: int, seed: int) -> Substrate:
     CACHE.mkdir(parents=True, exist_ok=True)
-    key = hashlib.sha1(f"axon_bundle-v1-{n_axons}-{seed}".encode()).hexdigest()[:16]
+    key = hashlib.sha1(f"axon_bundle-v2-{n_axons}-{seed}".encode()).hexdigest()[:16]
     path = CACHE / f"bundle_{key}.pkl"
     if path.exists():
         with open(path, "rb") as f:

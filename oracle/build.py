@@ -79,8 +79,11 @@ def build_reference_kernel(code: str) -> Path:
 REF_INDEX = REF_OUT / "index.json"
 
 # named CPU builds of the reference kernel that bench.py's reference arm loads
-# on a host without the reference tree: name -> walker count of the build
-BENCH_BUILDS = {"packed_cpu_16k": 16_000}
+# on a host without the reference tree: name -> (workload, walker count of the
+# build).  The batched benchmark's reference arm walks jobs 0, 16, 32 and 48
+# of the mixed workload with 8,000 walkers each.
+BENCH_BUILDS = {"packed_cpu_16k": ("packed_1e6", 16_000),
+                **{f"batched_job{i}_cpu_8k": (f"batched_job{i}", 8_000) for i in (0, 16, 32, 48)}}
 
 
 def build_reference_named(name: str, pars: dict) -> Path:
@@ -106,15 +109,16 @@ def reference_named(name: str):
 
 
 def build_reference_bench() -> list:
-    """The CPU builds of the reference kernel for bench.py's packed workload
-    (1 um cells; template constants as DiffSim3d forms them), where the
-    reference tree is present."""
+    """The CPU builds of the reference kernel for bench.py's reference arms
+    (the packed workload and a sample of the batched workload's jobs; 1 um
+    cells; template constants as DiffSim3d forms them), where the reference
+    tree is present."""
     if not reference_available():
         return []
     import sys
     sys.path.insert(0, str(ORACLE_DIR.parent))
     from baseline.reference_gpu import workload_pars
-    return [build_reference_named(name, workload_pars("packed_1e6", nspins=n)) for name, n in BENCH_BUILDS.items()]
+    return [build_reference_named(name, workload_pars(wl, nspins=n)) for name, (wl, n) in BENCH_BUILDS.items()]
 
 
 if __name__ == "__main__":

@@ -120,6 +120,7 @@ def test_empty_inputs_return_ok_without_gpu():
     assert lib.nz_phase_from_phi(by(empty), FAKE, 6, None, None) == 0
     assert lib.nz_moments(FAKE, FAKE, 0, FAKE, None) == 0
     assert lib.nz_cells_gather(FAKE, 4, None, 0, None, None, 512, FAKE, None, None) == 0
+    assert lib.nz_batch_sort(FAKE, 3, 0, 0, None, 0, None) == 0  # no walkers: nothing to do
     grid = sub.grid
     need = lib.nz_sort_scratch_bytes(0, 8 * 8 * 8)  # the histogram of the 8x8x8 grid's bins
     assert need > 0
@@ -160,6 +161,16 @@ def test_invalid_arguments_rejected_without_gpu():
     refused(lib.nz_phase_from_phi(by(a), FAKE, 6, None, None), "nz_phase_from_phi")
     refused(lib.nz_cells_gather(FAKE, 4, FAKE, 10, FAKE, FAKE, 0, FAKE, FAKE, None), "nz_cells_gather")
     refused(lib.nz_cells_gather(FAKE, 4, FAKE, 10, FAKE, FAKE, 8, FAKE + 4, FAKE, None), "nz_cells_gather")
+    # batched re-binning: key counts per job, scratch, walkers without keys or jobs
+    assert lib.nz_sort_job_keys(by(grid), 1, 0) == 512 and lib.nz_sort_job_keys(by(grid), 3, 5) == 27 * 5
+    assert lib.nz_sort_job_keys(by(bad_grid), 1, 0) == -1 and lib.nz_sort_job_keys(by(grid), 0, 0) == -1
+    assert lib.nz_batch_sort_scratch_bytes(N, 3 * nb) == lib.nz_sort_scratch_bytes(N, 3 * nb)
+    bneed = lib.nz_batch_sort_scratch_bytes(N, 3 * nb)
+    refused(lib.nz_batch_sort(FAKE, 3, N, 3 * nb, FAKE, bneed - 4, None), "nz_batch_sort", _lib.NZ_ERR_CAPACITY)
+    refused(lib.nz_batch_sort(FAKE, 3, N, 0, FAKE, bneed, None), "nz_batch_sort")
+    refused(lib.nz_batch_sort(FAKE, 0, N, 3 * nb, FAKE, bneed, None), "nz_batch_sort")
+    refused(lib.nz_batch_sort(None, 3, N, 3 * nb, FAKE, bneed, None), "nz_batch_sort")
+    refused(lib.nz_batch_sort(FAKE, 3, -1, 3 * nb, FAKE, bneed, None), "nz_batch_sort")
     # fused walk: draw table, step range, moments limits, misaligned cell records
     refused(lib.nz_walk_fused(by(sub), by(a), _lib.MODE_PHI, 0.01, FAKE, FAKE, 0, 10,
                               by(_lib.Draws(FAKE, 10, 4, 1, 2, 0)), None, None), "nz_walk_fused")

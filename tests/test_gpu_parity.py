@@ -403,3 +403,63 @@ def test_sort_with_many_bins(eng):
         np.testing.assert_array_equal(rec, rec0)
         key = cell if nlabels == 0 else label.astype(np.int64) * 128000 + cell  # label * bins + bin
         assert np.all(np.diff(key) >= 0)
+
+
+def test_batch_sort_equals_per_job_sorts(eng):
+    """One re-binning pass over three jobs of different grids, walker counts
+    and label counts (nz_batch_sort): each job's output is a permutation of
+    its own walkers, records intact, in non-decreasing (label, bin) or bin
+    order of its own grid, as nz_state_sort_keyed leaves them."""
+    import ctypes
+    from nozomi_b200 import _lib as L
+    from nozomi_b200.batch import _sort_table
+    rng = np.random.default_rng(22)
+    cases = [((40.0, 40.0, 80.0), (40, 40, 80), 2, 3, 70_001),
+             ((12.0, 9.0, 20.0), (12, 9, 20), 4, 0, 5_000),
+             ((30.0, 30.0, 30.0), (60, 60, 60), 8, 7, 131_072)]
+    jobs, pairs = [], []
+    for L3, nseg, coarsen, nl, N in cases:
+        pos = np.stack([rng.uniform(-L3[a] / 2, L3[a] / 2, N) for a in range(3)]).astype(np.float32)
+        lab = rng.integers(-1, max(nl, 1) + 1, N).astype(np.int32)
+        x = _dev(pos)
+        wk = eng.Walkers(x, x + 0.5, phi=_dev(rng.normal(0, 1, (6, N)).astype(np.float32)), label=_dev(lab))
+        src, dst = eng.FusedState.from_walkers(wk), eng.FusedState(N)
+        sub = type("S", (), {"grid": eng.box_grid(L3, nseg), "nstructures": max(nl - 1, 0)})()
+        jobs.append((L3, nseg, coarsen, nl, src, dst))
+        pairs.append(({"sub": sub}, src, dst))
+    # nlabels per job as the table builder would set them (nstructures + 1 when by label)
+    table, n, tw, tk = _sort_table(pairs, 1, True)
+    raw = bytearray(table.cpu().numpy().tobytes())
+    arr = (L.SortJob * n).from_buffer(raw)
+    for i, (L3, nseg, coarsen, nl, src, dst) in enumerate(jobs):
+        arr[i].coarsen, arr[i].nlabels = coarsen, nl
+    tk = 0
+    for i, (L3, nseg, coarsen, nl, src, dst) in enumerate(jobs):
+        arr[i].key_offset = tk
+        tk += int(L.load().nz_sort_job_keys(L.byref(arr[i].grid), coarsen, nl))
+    table = torch.from_numpy(np.frombuffer(bytes(raw), dtype=np.uint8).copy()).cuda()
+    scratch = torch.empty(int(L.load().nz_batch_sort_scratch_bytes(tw, tk)), dtype=torch.uint8, device="cuda")
+    L.check(L.load().nz_batch_sort(ctypes.c_void_p(table.data_ptr()), n, tw, tk, ctypes.c_void_p(scratch.data_ptr()),
+                                   scratch.numel(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+            "nz_batch_sort")
+    torch.cuda.synchronize()
+    for L3, nseg, coarsen, nl, src, dst in jobs:
+        rec = lambda st: np.concatenate([getattr(st, t).cpu().numpy() for t in ("pos", "org", "phi", "comp")], 1)  # noqa: E731
+        a, b = rec(src), rec(dst)
+        ia, ib = a[:, 7].view(np.int32), b[:, 7].view(np.int32)
+        np.testing.assert_array_equal(np.sort(ib), np.arange(src.N))
+        np.testing.assert_array_equal(a[np.argsort(ia)], b[np.argsort(ib)])
+        p = b[:, :3].astype(np.float32)
+        idx = []
+        for ax in range(3):
+            half, d = np.float32(L3[ax] / 2), np.float32(L3[ax] / nseg[ax])
+            c = np.floor((p[:, ax] + half) / d)
+            idx.append(np.clip(c, 0, nseg[ax] - 1).astype(np.int64) // coarsen)
+        bx, by = -(-nseg[0] // coarsen), -(-nseg[1] // coarsen)
+        nbins = bx * by * -(-nseg[2] // coarsen)
+        key = (idx[2] * by + idx[1]) * bx + idx[0]
+        if nl > 0:
+            lab = b[:, 3].view(np.int32).astype(np.int64)
+            lab = np.where((lab < 0) | (lab >= nl), nl - 1, lab)
+            key = key + lab * nbins
+        assert np.all(np.diff(key) >= 0)

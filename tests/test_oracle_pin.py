@@ -120,11 +120,11 @@ def _packed_reference():
     from oracle.cells_oracle import padded_as_lists
     sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
     import bench
-    if reference_named(bench.REF_CPU_BUILD) is None:
+    if reference_named("packed_cpu_16k") is None:
         pytest.skip("oracle/_ref reference build absent (the reference tree was absent at build)")
-    sub, pg, dirs, _ = bench.workload()
-    ref = bench.ReferenceCpu(sub, pg, dirs)
-    _, pars = reference_named(bench.REF_CPU_BUILD)
+    sub, pg, dirs, _ = bench.workload_packed()
+    ref = bench.ReferenceCpu("packed_cpu_16k", sub, pg, dirs)
+    _, pars = reference_named("packed_cpu_16k")
     nseg = (int(pars["nLx"]), int(pars["nLy"]), int(pars["nLz"]))
     st, ct, it = padded_as_lists(ref.K, ref.seg, nseg[0] * nseg[1] * nseg[2])
     ns = sub.nstructures

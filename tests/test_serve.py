@@ -26,7 +26,8 @@ def test_served_equals_alone():
     specs = [_spec(i, na, N, st, nd) for i, (na, N, st, nd) in
              enumerate([(10, 3000, 600, 6), (20, 5000, 400, 9), (15, 2048, 900, 7), (12, 4000, 300, 12),
                         (10, 1000, 750, 8)])]
-    srv = Server(tuning=tuning, threads=128)
+    # fixed 150-step rounds, so the requests overlap over several rounds
+    srv = Server(tuning=tuning, threads=128, min_steps=150, max_steps=150)
     tickets = [srv.submit(specs[0]), srv.submit(specs[1])]
     srv.round()                       # two requests running
     tickets.append(srv.submit(specs[2]))
@@ -42,21 +43,55 @@ def test_served_equals_alone():
 
 
 def test_admission_by_memory_budget():
+    """With a substrate cache of its own budget, requests are admitted into
+    all of hbm_budget: two of four fit at once.  Without one, the server's
+    own cache takes a quarter and requests the rest."""
+    from nozomi_b200.batch import SubstrateCache
     from nozomi_b200.serve import Server, footprint
     from nozomi_b200.simulate import Tuning
     tuning = Tuning(steps_per_launch=200)
     specs = [_spec(i, 10, 4000, 400, 6) for i in range(4)]
     budget = footprint(specs[0], tuning) + footprint(specs[1], tuning) + 1
-    srv = Server(tuning=tuning, hbm_budget=budget)
+    srv = Server(tuning=tuning, hbm_budget=budget, cache=SubstrateCache())
     for sp in specs:
         srv.submit(sp)
     peak = 0
-    while srv.waiting or srv.active:
+    while srv.waiting or srv.resident:
         srv._admit()
-        peak = max(peak, len(srv.active))
+        peak = max(peak, len(srv.resident))
         assert srv.used <= budget
         srv.round()
     assert peak == 2 and len(srv.done) == 4
+    own = Server(tuning=tuning, hbm_budget=4 * budget)
+    assert own.cache.budget == budget and own.budget == 3 * budget
+
+
+def test_requests_arriving_during_a_round_are_staged_then_served():
+    """The request loop admits arrivals while a round runs on the GPU: their
+    set-up goes to the side stream, they join a later round, and every result
+    equals the request alone (time-bounded rounds, chunk sizes vary)."""
+    from nozomi_b200.batch import BatchRun, SubstrateCache
+    from nozomi_b200.serve import Server
+    from nozomi_b200.simulate import Tuning
+    from nozomi_b200.workloads import Request
+    tuning = Tuning(steps_per_launch=200)
+    specs = [_spec(i, 10 + 3 * i, 20000, 1500, 6 + i) for i in range(4)]
+    srv = Server(tuning=tuning, threads=128, round_s=0.01, min_steps=50)
+    staged_seen = []
+    real_admit = srv._admit
+
+    def admit():
+        real_admit()
+        staged_seen.append(len(srv.staged))
+    srv._admit = admit
+    reqs = [Request(0.0, specs[0]), Request(0.0, specs[1]), Request(0.05, specs[2]), Request(0.1, specs[3])]
+    done = srv.serve(reqs)
+    assert len(done) == 4 and all(t.error is None for t in done)
+    assert max(staged_seen) >= 1 and srv.rounds >= 3
+    cache = SubstrateCache()
+    for t in done:
+        alone = BatchRun([t.spec], tuning=tuning, threads=64, cache=cache).step().signals()[0]
+        np.testing.assert_allclose(t.signal, alone, rtol=0, atol=1e-12)
 
 
 def test_bad_request_fails_alone():
