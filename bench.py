@@ -115,6 +115,9 @@ def parse(argv=None):
     ap.add_argument("--coarsen", type=int, default=None)
     ap.add_argument("--by-label", type=int, default=None, help="re-bin by (label, bin): 1, or by bin only: 0")
     ap.add_argument("--near-margin", type=float, default=None, help="near-list margin in um (0: none)")
+    ap.add_argument("--lists", default=None, choices=["index", "records"],
+                    help="the fused walk's list form: index (16/32-bit entries into one record array) or records "
+                         "(per-entry sphere records)")
     ap.add_argument("--narrow-walkers", type=float, default=5e5, help="narrow: walkers")
     ap.add_argument("--narrow-ms", type=float, default=100.0, help="narrow: simulated time, ms")
     ap.add_argument("--serve", default="5:30,20:10",
@@ -497,24 +500,16 @@ def run_packed(args):
     sub, pg, dirs, bvals = workload_packed()
     # launch shape tuned for this workload by sweeps on a B200: 0.5 um cells,
     # near margin 0.5 um, re-binning bins of 8^3 cells, 2000 steps per launch
-    tuning = Tuning(cell=0.5, near_margin=0.5, coarsen=8, steps_per_launch=2000)
-    if args.cell:
-        tuning.cell = args.cell
-    if args.steps_per_launch:
-        tuning.steps_per_launch = args.steps_per_launch
-    if args.coarsen:
-        tuning.coarsen = args.coarsen
-    if args.by_label is not None:
-        tuning.by_label = bool(args.by_label)
-    if args.near_margin is not None:
-        tuning.near_margin = args.near_margin if args.near_margin > 0 else None
-    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin)
+    tuning = _tuning_from_args(args, Tuning(cell=0.5, near_margin=0.5, coarsen=8, steps_per_launch=2000))
+    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin,
+                            lists=tuning.lists)
     # the one-time cell build (member lists, near lists, per-entry records) is
     # outside the metric; it is timed on a second build, the first having
     # loaded the library and warmed the allocator
     torch.cuda.synchronize()
     tb = time.perf_counter()
-    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin)
+    dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin,
+                            lists=tuning.lists)
     torch.cuda.synchronize()
     cell_build_ms = (time.perf_counter() - tb) * 1e3
     amps = pg.amplitude_for_b(bvals)
@@ -654,7 +649,8 @@ def run_packed(args):
                 "config": {"workload": WORKLOAD, "walkers_per_gpu": N, "time_steps": run.nsteps,
                            "directions": int(dirs.shape[1]), "bvalues": bvals.tolist(),
                            "cell_um": tuning.cell, "steps_per_launch": tuning.steps_per_launch,
-                           "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label, "near_margin_um": tuning.near_margin,
+                           "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label,
+                           "near_margin_um": tuning.near_margin, "lists": tuning.lists,
                            "near_list_entries": int(dsub.near[2].numel()) if dsub.near is not None else 0,
                            "spheres": sub.S, "cells": dsub.ncell,
                            "cell_list_entries": dsub.n_items, "l2": "256 MiB flush between timed steps",
@@ -694,6 +690,8 @@ def _tuning_from_args(args, base):
         base.by_label = bool(args.by_label)
     if args.near_margin is not None:
         base.near_margin = args.near_margin if args.near_margin > 0 else None
+    if args.lists:
+        base.lists = args.lists
     return base
 
 
@@ -871,7 +869,7 @@ def run_batched(args):
               "walkers": sum(sp.N for sp in all_specs), "threads": threads,
               "steps_per_launch": tuning.steps_per_launch, "near_margin_um": tuning.near_margin,
               "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label,
-              "persistent_grid": run.grid, "chunks": len(run.chunks),
+              "lists": tuning.lists, "persistent_grid": run.grid, "chunks": len(run.chunks),
               "l2": "256 MiB flush between timed steps (the inputs, 64 substrates' cell lists and walker "
                     "state, are also larger than L2)",
               "parallelism": (f"jobs sharded whole over {world} GPUs, longest first" if world > 1 else "one GPU")}

@@ -40,6 +40,11 @@ extern "C" {
 #define NZ_MODE_TANGENT64 16 /* fused walk: a solve whose normalised discriminant sqterm/4a is below
                                 1e-6 um^2 (a near-tangent ray) is recomputed in FP64 */
 
+/* list format of every job of one nz_walk_batch launch (mode bits; none: the
+ * per-entry record lists) */
+#define NZ_LIST_IDX16 64    /* substrates with idx_bytes 2 */
+#define NZ_LIST_IDX32 128   /* substrates with idx_bytes 4 */
+
 /* per-walker flag bits */
 #define NZ_FLAG_DRAWS_EXHAUSTED 1
 #define NZ_FLAG_ITER_CAP 2
@@ -81,6 +86,24 @@ typedef struct nz_substrate {
     const int* near_count;
     const float* near_sph4;
     const int* near_sid;
+    /* Index form of the fused walk's lists (idx_bytes 2 or 4; 0: the
+     * per-entry records above, which may then be NULL).  The spheres are put
+     * in record order -- sorted by structure id, stable -- and rec4 holds
+     * their (cx, cy, cz, r), rec_sid their structure ids; sid_start[k]
+     * (k = 0 .. nstructures + 1) is the first record of a structure >= k
+     * (sid_start[nstructures] = sid_start[nstructures + 1] = S).  A list
+     * entry is a record index (uint16_t when idx_bytes is 2, int32 when 4),
+     * ascending within a cell, laid out by the same cell_start / cell_count
+     * (near_start / near_count for near_idx) as the record lists
+     * (nz_cells_index).  Entries ascending by record are ascending by
+     * structure, so a walker labelled L stops at the first record at or
+     * beyond sid_start[L + 1]: no structure id is read per entry. */
+    int idx_bytes;
+    const void* cell_idx;
+    const void* near_idx;
+    const float* rec4;         /* [S][4], 16-byte aligned */
+    const int* rec_sid;        /* [S] */
+    const int* sid_start;      /* [nstructures + 2] */
 } nz_substrate;
 
 /* Source of the normal draws: an injected table normals[N][nsteps][maxk]
@@ -176,6 +199,13 @@ int nz_segments_fill(const double* spheres64, int S, double Lx, double Ly, doubl
 int nz_cells_gather(const float* spheres, int S, const int* items, int n_items, const int* cell_start,
                     const int* cell_count, int ncell, float* sph4, int* sid, void* stream);
 
+/* Index lists of the fused walk: idx[k] = perm[items[k]] (perm: the record
+ * index of every sphere, [S]; NULL = identity), then each cell's entries
+ * sorted ascending.  idx_bytes 2 (uint16_t entries; needs S <= 65536) or 4
+ * (int32). */
+int nz_cells_index(const int* items, int n_items, const int* perm, int S, const int* cell_start,
+                   const int* cell_count, int ncell, void* idx, int idx_bytes, void* stream);
+
 /* ---- a7: seeding — seedSpinsKernel (sim3d_kernel.cu:240-337) + SimGeometry3D.gpu_seed
  * (geometry.py:73-174).  target[k] != 0 marks structure k (k = nstructures is the
  * box) as a target.  A position is accepted when the first structure in id order
@@ -236,9 +266,11 @@ int nz_walk_fused_moments(const nz_substrate* sub, const nz_state* st, int mode,
  * (0 = one CTA per item, no queue); threads = walkers per CTA (a multiple of
  * 32 up to 256); an item holds at most `threads` walkers.  The batched form of
  * the fused walk: many substrates, protocols and walker sets in one launch.
+ * mode may carry NZ_LIST_IDX16 or NZ_LIST_IDX32: every job's substrate then
+ * has index lists of that width (otherwise every job's has record lists).
  * The device arrays are not read back for checking: the caller guarantees
- * 0 <= item.job < n_jobs, 1 <= item.count <= threads and
- * item.first + item.count <= that job's state.N. */
+ * 0 <= item.job < n_jobs, 1 <= item.count <= threads,
+ * item.first + item.count <= that job's state.N, and the list format. */
 int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0, int step1,
                   int* queue, int grid, int threads, void* stream);
 

@@ -12,6 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libnozomi_b200.so"
 
 NZ_OK, NZ_ERR_ARG, NZ_ERR_CUDA, NZ_ERR_CAPACITY, NZ_ERR_UNSEEDED = 0, 1, 2, 3, 4
 MODE_SIG, MODE_PHASE, MODE_PHI, MODE_MOMENTS, MODE_TANGENT64 = 1, 2, 4, 8, 16
+LIST_IDX16, LIST_IDX32 = 64, 128  # nz_walk_batch: the jobs' list format (none: per-entry records)
 FLAG_DRAWS_EXHAUSTED, FLAG_ITER_CAP, FLAG_UNSEEDED = 1, 2, 4
 FUSED_THREADS = 128       # walkers per CTA / per work item of the fused and batched walks
 MOMENT_STEPS = 256        # steps per launch when the fused walk accumulates moments
@@ -33,7 +34,8 @@ class Substrate(ctypes.Structure):
     _fields_ = [("grid", Grid), ("nstructures", _i), ("S", _i), ("spheres", _P), ("cell_start", _P),
                 ("cell_count", _P), ("cell_items", _P), ("cell_sph4", _P), ("cell_sid", _P), ("D", _P),
                 ("T2", _P), ("near_margin", _f), ("near_start", _P), ("near_count", _P), ("near_sph4", _P),
-                ("near_sid", _P)]
+                ("near_sid", _P), ("idx_bytes", _i), ("cell_idx", _P), ("near_idx", _P), ("rec4", _P),
+                ("rec_sid", _P), ("sid_start", _P)]
 
 
 class Draws(ctypes.Structure):
@@ -74,6 +76,7 @@ SIGNATURES = {
     "nz_cells_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _d, _P, _P, _P, _P, _P]),
     "nz_segments_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _i, _P, _P]),
     "nz_cells_gather": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _P, _P]),
+    "nz_cells_index": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _i, _P]),
     "nz_seed": (_i, [_P, _P, _i, _u, _u, _u, _i, _P, _P, _P, _P]),
     "nz_seed_range": (_i, [_P, _P, _u, _i, _u, _u, _u, _i, _P, _P, _P, _P]),
     "nz_walk_step": (_i, [_P, _P, _i, _f, _f, _f, _i, _P, _P]),

@@ -71,14 +71,15 @@ class SubstrateCache:
         self.misses = 0
 
     def get(self, key, substrate: Substrate, D, T2, tuning: Tuning) -> engine.DeviceSubstrate:
-        k = (key, float(D), float(T2), tuning.cell, tuning.near_margin)
+        k = (key, float(D), float(T2), tuning.cell, tuning.near_margin, tuning.lists)
         if k in self.items:
             self.hits += 1
             self.order.remove(k)
             self.order.append(k)
             return self.items[k]
         self.misses += 1
-        d = device_substrate(substrate, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin)
+        d = device_substrate(substrate, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin,
+                             lists=tuning.lists)
         self.items[k] = d
         self.hosts[k] = substrate
         self.order.append(k)
@@ -135,6 +136,28 @@ def _sort_table(pairs, coarsen, by_label):
     return torch.from_numpy(raw).cuda(), len(pairs), tw, tk
 
 
+LIST_BITS = {0: 0, 2: L.LIST_IDX16, 4: L.LIST_IDX32}
+
+
+def list_groups(jobs, active) -> dict:
+    """Active jobs by the list form of their substrate (idx_bytes): one
+    batched launch per form."""
+    groups = {}
+    for i in active:
+        groups.setdefault(jobs[i]["sub"].idx_bytes, []).append(i)
+    return groups
+
+
+def batch_grid(threads: int, lk: int) -> int:
+    """Persistent grid of the batched walk: CTAs resident per SM x SMs."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    occ = ctypes.c_int(0)
+    L.check(L.load().nz_batch_occupancy(L.MODE_PHI | LIST_BITS[lk], int(threads), ctypes.byref(occ)),
+            "nz_batch_occupancy")
+    return sms * max(1, occ.value)
+
+
 def _items(jobs, active, threads, s0, k) -> torch.Tensor:
     """Items (job, first walker, count) of the active jobs, longest remaining
     work first (ties in job, then walker order)."""
@@ -182,10 +205,8 @@ class BatchRun:
         # and amplitudes above, plus positions given as host arrays and the
         # chunk tables (added by prepare)
         self.h2d_bytes = sum(j["G"].numel() * 8 + j["dirs"].numel() * 4 + j["amps"].numel() * 4 for j in self.jobs)
-        sms = torch.cuda.get_device_properties(dev).multi_processor_count
-        occ = ctypes.c_int(0)
-        L.check(L.load().nz_batch_occupancy(L.MODE_PHI, self.threads, ctypes.byref(occ)), "nz_batch_occupancy")
-        self.grid = sms * max(1, occ.value)
+        self.grids = {lk: batch_grid(self.threads, lk) for lk in {j["sub"].idx_bytes for j in self.jobs}}
+        self.grid = max(self.grids.values())
         self._planned = False
 
     # -- set-up ------------------------------------------------------------------
@@ -242,15 +263,19 @@ class BatchRun:
             states = [self.jobs[i]["buf"][cur[i]] for i in range(len(self.jobs))]
             sort, n_sort, tw, tk = _sort_table(pairs, self.tuning.coarsen, self.tuning.by_label)
             need = max(need, int(L.load().nz_batch_sort_scratch_bytes(tw, tk)))
-            items = _items(self.jobs, active, self.threads, s0, k)
+            launches = []
+            for lk, grp in sorted(list_groups(self.jobs, active).items()):
+                items = _items(self.jobs, grp, self.threads, s0, k)
+                launches.append((lk, items))
+                self.h2d_bytes += items.numel() * 4
             ws = sum(min(k, self.jobs[i]["nsteps"] - s0) * self.jobs[i]["N"] for i in active)
             self.chunks.append({"s0": s0, "s1": s0 + k, "active": active, "table": _job_table(self.jobs, states),
-                                "items": items, "sort": sort, "n_sort": n_sort, "sort_walkers": tw,
+                                "launches": launches, "sort": sort, "n_sort": n_sort, "sort_walkers": tw,
                                 "sort_keys": tk, "walker_steps": ws})
-            self.h2d_bytes += sort.numel() + items.numel() * 4 + self.chunks[-1]["table"].numel()
+            self.h2d_bytes += sort.numel() + self.chunks[-1]["table"].numel()
         self.final_cur = cur
         self.sort_scratch = torch.empty(max(need, 1), dtype=torch.uint8, device="cuda")
-        self.queue = torch.zeros(len(self.chunks), dtype=torch.int32, device="cuda")
+        self.queue = torch.zeros(3 * len(self.chunks), dtype=torch.int32, device="cuda")
         self.out = [torch.zeros((2, j["dirs"].shape[1], j["amps"].numel()), dtype=torch.float64, device="cuda")
                     for j in self.jobs]
         self._planned = True
@@ -271,10 +296,12 @@ class BatchRun:
             if events is not None:
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(cs)
-            L.check(lib.nz_walk_batch(ctypes.c_void_p(c["table"].data_ptr()), len(self.jobs),
-                                      ctypes.c_void_p(c["items"].data_ptr()), int(c["items"].shape[0]), L.MODE_PHI,
-                                      c["s0"], c["s1"], ctypes.c_void_p(self.queue.data_ptr() + 4 * qi), self.grid,
-                                      self.threads, stream), "nz_walk_batch")
+            for g, (lk, items) in enumerate(c["launches"]):
+                L.check(lib.nz_walk_batch(ctypes.c_void_p(c["table"].data_ptr()), len(self.jobs),
+                                          ctypes.c_void_p(items.data_ptr()), int(items.shape[0]),
+                                          L.MODE_PHI | LIST_BITS[lk], c["s0"], c["s1"],
+                                          ctypes.c_void_p(self.queue.data_ptr() + 4 * (3 * qi + g)), self.grids[lk],
+                                          self.threads, stream), "nz_walk_batch")
             if events is not None:
                 e1.record(cs)
                 events.append((e0, e1))
@@ -296,7 +323,7 @@ class BatchRun:
         for c in self.chunks:
             if c["sort_walkers"]:
                 n += 2 + (1 if c["sort_keys"] <= L.SCAN_SINGLE_KEYS else 3)
-            n += 1 if c["items"].shape[0] else 0
+            n += sum(1 for _, items in c["launches"] if items.shape[0])
         return n
 
     def signals(self) -> list:

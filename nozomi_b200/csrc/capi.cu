@@ -158,6 +158,18 @@ extern "C" int nz_state_unpack_by_id(const nz_state* st, const nz_walkers* wk, i
 static int check_fused_sub(const nz_substrate* sub, const char* who) {
   int rc = check_substrate(sub, who);
   if (rc) return rc;
+  if (sub->idx_bytes != 0) {
+    if (sub->idx_bytes != 2 && sub->idx_bytes != 4)
+      return set_error(NZ_ERR_ARG, "%s: idx_bytes %d is not 0, 2 or 4", who, sub->idx_bytes);
+    if (sub->idx_bytes == 2 && sub->S > 65536)
+      return set_error(NZ_ERR_ARG, "%s: %d spheres do not fit 16-bit indices", who, sub->S);
+    if (!sub->cell_idx || !sub->rec4 || !sub->rec_sid || !sub->sid_start)
+      return set_error(NZ_ERR_ARG, "%s: index lists need cell_idx, rec4, rec_sid and sid_start", who);
+    if (!aligned16(sub->rec4)) return set_error(NZ_ERR_ARG, "%s: rec4 must be 16-byte aligned", who);
+    if (sub->near_idx && (!sub->near_start || !sub->near_count || !(sub->near_margin > 0.0f)))
+      return set_error(NZ_ERR_ARG, "%s: incomplete near lists", who);
+    return NZ_OK;
+  }
   if (!sub->cell_sph4 || !sub->cell_sid) return set_error(NZ_ERR_ARG, "%s: substrate lacks cell_sph4/cell_sid", who);
   if (!aligned16(sub->cell_sph4)) return set_error(NZ_ERR_ARG, "%s: cell_sph4 must be 16-byte aligned", who);
   if (sub->near_sph4) {
@@ -166,6 +178,12 @@ static int check_fused_sub(const nz_substrate* sub, const char* who) {
     if (!aligned16(sub->near_sph4)) return set_error(NZ_ERR_ARG, "%s: near_sph4 must be 16-byte aligned", who);
   }
   return NZ_OK;
+}
+
+// List kind of an nz_walk_batch launch from its mode bits.
+static int batch_list_kind(int mode) {
+  if ((mode & NZ_LIST_IDX16) && (mode & NZ_LIST_IDX32)) return -1;
+  return (mode & NZ_LIST_IDX16) ? 2 : (mode & NZ_LIST_IDX32) ? 4 : 0;
 }
 
 extern "C" int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mode, float dt, const float* G,
@@ -187,8 +205,8 @@ extern "C" int nz_walk_fused(const nz_substrate* sub, const nz_state* st, int mo
   if (st->N == 0 || step1 == step0) return NZ_OK;
   const JobDev j = make_job(*sub, G, Garea, step1, dt, *draws, mode, *st, moments);
   const int n_items = (st->N + kFusedThreads - 1) / kFusedThreads;
-  return launch_fused(mode, j, nullptr, nullptr, n_items, step0, step1, nullptr, n_items, kFusedThreads,
-                      static_cast<cudaStream_t>(stream));
+  return launch_fused(mode, sub->idx_bytes, j, nullptr, nullptr, n_items, step0, step1, nullptr, n_items,
+                      kFusedThreads, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" size_t nz_walk_fused_moments_scratch_bytes(int N, int nsteps) {
@@ -217,7 +235,8 @@ extern "C" int nz_walk_fused_moments(const nz_substrate* sub, const nz_state* st
   JobDev j = make_job(*sub, G, Garea, step1, dt, *draws, mode, *st, nullptr);
   j.disp = scratch;
   const int n_items = (st->N + kFusedThreads - 1) / kFusedThreads;
-  rc = launch_fused(mode | kModeDisp, j, nullptr, nullptr, n_items, step0, step1, nullptr, n_items, kFusedThreads, cs);
+  rc = launch_fused(mode | kModeDisp, sub->idx_bytes, j, nullptr, nullptr, n_items, step0, step1, nullptr, n_items,
+                    kFusedThreads, cs);
   if (rc) return rc;
   const int gx = min(64, (st->N + 255) / 256);
   disp_moments_kernel<<<dim3(gx, step1 - step0), 256, 0, cs>>>(scratch, st->N, moments + size_t(step0) * 6);
@@ -233,14 +252,18 @@ extern "C" int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* item
                      kFusedMaxThreads);
   if (grid > 0 && !queue) return set_error(NZ_ERR_ARG, "nz_walk_batch: a persistent grid needs a queue counter");
   if (mode & NZ_MODE_MOMENTS) return set_error(NZ_ERR_ARG, "nz_walk_batch: moments are per-substrate (nz_walk_fused)");
+  const int lk = batch_list_kind(mode);
+  if (lk < 0) return set_error(NZ_ERR_ARG, "nz_walk_batch: both list widths in mode %d", mode);
   if (n_items == 0 || step1 == step0) return NZ_OK;
   const JobDev unused{};
-  return launch_fused(mode, unused, jobs, items, n_items, step0, step1, grid > 0 ? queue : nullptr,
-                      grid > 0 ? grid : n_items, threads, static_cast<cudaStream_t>(stream));
+  return launch_fused(mode & ~(NZ_LIST_IDX16 | NZ_LIST_IDX32), lk, unused, jobs, items, n_items, step0, step1,
+                      grid > 0 ? queue : nullptr, grid > 0 ? grid : n_items, threads,
+                      static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int nz_batch_occupancy(int mode, int threads, int* blocks_per_sm) {
-  if (!blocks_per_sm || threads < 32 || threads > kFusedMaxThreads)
+  const int lk = batch_list_kind(mode);
+  if (!blocks_per_sm || threads < 32 || threads > kFusedMaxThreads || lk < 0)
     return set_error(NZ_ERR_ARG, "nz_batch_occupancy: bad arguments");
-  return occupancy_fused(mode, threads, blocks_per_sm);
+  return occupancy_fused(mode & ~(NZ_LIST_IDX16 | NZ_LIST_IDX32), lk, threads, blocks_per_sm);
 }

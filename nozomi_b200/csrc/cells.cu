@@ -272,6 +272,52 @@ __global__ void gather_records_kernel(const float* __restrict__ spheres, int S, 
   sph4[k] = make_float4(spheres[s], spheres[S + s], spheres[2 * S + s], spheres[3 * S + s]);
 }
 
+// Index lists: each entry becomes its sphere's record index, then each
+// cell's entries are sorted ascending (a heapsort per cell; one thread per
+// cell).  Sphere order within the reference layout is usually already by
+// structure, so the sort mostly finds its input in order.
+template <typename T>
+__global__ void index_fill_kernel(const int* __restrict__ items, int n, const int* __restrict__ perm,
+                                  T* __restrict__ idx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int s = items[k];
+  idx[k] = T(perm ? perm[s] : s);
+}
+
+template <typename T>
+__global__ void index_sort_kernel(const int* __restrict__ start, const int* __restrict__ count, int ncell,
+                                  T* __restrict__ idx) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  T* a = idx + start[c];
+  const int n = count[c];
+  bool sorted = true;
+  for (int i = 1; i < n && sorted; ++i) sorted = a[i - 1] <= a[i];
+  if (sorted) return;
+  auto sift = [&](int root, int end) {
+    while (2 * root + 1 < end) {
+      int child = 2 * root + 1;
+      if (child + 1 < end && a[child] < a[child + 1]) child++;
+      if (a[root] < a[child]) {
+        const T t = a[root];
+        a[root] = a[child];
+        a[child] = t;
+        root = child;
+      } else {
+        return;
+      }
+    }
+  };
+  for (int i = n / 2 - 1; i >= 0; --i) sift(i, n);
+  for (int end = n - 1; end > 0; --end) {
+    const T t = a[0];
+    a[0] = a[end];
+    a[end] = t;
+    sift(0, end);
+  }
+}
+
 // Exclusive scan of in[lo, hi) into out[lo, hi) by one CTA (1024 threads, 8
 // items per thread per pass), starting from carry; returns the range's total
 // (in every thread).
@@ -439,4 +485,30 @@ extern "C" int nz_cells_gather(const float* spheres, int S, const int* items, in
   if (rc) return rc;
   gather_records_kernel<<<(n_items + 255) / 256, 256, 0, st>>>(spheres, S, n_items, s4);
   return check_launch("gather_records_kernel");
+}
+
+extern "C" int nz_cells_index(const int* items, int n_items, const int* perm, int S, const int* cell_start,
+                              const int* cell_count, int ncell, void* idx, int idx_bytes, void* stream) {
+  if (n_items < 0 || ncell < 0 || S < 0 || (idx_bytes != 2 && idx_bytes != 4) ||
+      (n_items > 0 && (!items || !idx || !cell_start || !cell_count || ncell == 0)))
+    return set_error(NZ_ERR_ARG, "nz_cells_index: bad arguments (items=%d cells=%d idx_bytes=%d)", n_items, ncell,
+                     idx_bytes);
+  if (idx_bytes == 2 && S > 65536)
+    return set_error(NZ_ERR_ARG, "nz_cells_index: %d spheres do not fit 16-bit indices", S);
+  if (n_items == 0) return NZ_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (idx_bytes == 2) {
+    auto* p = static_cast<uint16_t*>(idx);
+    index_fill_kernel<uint16_t><<<(n_items + 255) / 256, 256, 0, st>>>(items, n_items, perm, p);
+    int rc = check_launch("index_fill_kernel");
+    if (rc) return rc;
+    index_sort_kernel<uint16_t><<<(ncell + 127) / 128, 128, 0, st>>>(cell_start, cell_count, ncell, p);
+  } else {
+    auto* p = static_cast<int*>(idx);
+    index_fill_kernel<int><<<(n_items + 255) / 256, 256, 0, st>>>(items, n_items, perm, p);
+    int rc = check_launch("index_fill_kernel");
+    if (rc) return rc;
+    index_sort_kernel<int><<<(ncell + 127) / 128, 128, 0, st>>>(cell_start, cell_count, ncell, p);
+  }
+  return check_launch("index_sort_kernel");
 }

@@ -52,11 +52,7 @@ constexpr int kFusedMaxThreads = 256;  // largest CTA of nz_walk_batch
 #ifndef NZ_FUSED_MIN_BLOCKS
 #define NZ_FUSED_MIN_BLOCKS 3
 #endif
-#ifndef NZ_SCAN_BATCH
-#define NZ_SCAN_BATCH 1
-#endif
 constexpr int kFusedMinBlocks = NZ_FUSED_MIN_BLOCKS;  // 256-thread CTAs per SM the register budget is sized for
-constexpr int kScanBatch = NZ_SCAN_BATCH;             // cell-list entries loaded together per thread
 constexpr int kMomentSteps = 256;  // steps per launch in NZ_MODE_MOMENTS (shared-memory staging)
 // Internal mode bit (nz_walk_fused_moments only): at each step end the fused
 // walk stores the walker's float displacement from its origin; a reduction
@@ -86,19 +82,27 @@ struct JobDev {
   float* disp;  // kModeDisp: per-step displacements [steps of the launch][3][nwalkers]
   int nwalkers;
   int step_offset;
-  // near lists (null sph4: none)
+  // near lists (null sph4, or null near_idx in index form: none)
   float near_margin;
   const int* near_start;
   const int* near_count;
   const float4* near_sph4;
   const int* near_sid;
+  // index form of the lists (nz_substrate.idx_bytes > 0)
+  const void* idx;
+  const void* near_idx;
+  const float4* rec4;
+  const int* rec_sid;
+  const int* sid_start;
+  int S;
 };
 
 __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, const float* Garea, int nsteps, float dt,
                                     const nz_draws& d, int mode, const nz_state& st, double* moments);
-int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
-                 int step1, int* queue, int grid, int threads, cudaStream_t st);
-int occupancy_fused(int mode, int threads, int* blocks_per_sm);
+// lk: list kind, 0 (per-entry records), 2 or 4 (index lists of that width)
+int launch_fused(int mode, int lk, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items,
+                 int step0, int step1, int* queue, int grid, int threads, cudaStream_t st);
+int occupancy_fused(int mode, int lk, int threads, int* blocks_per_sm);
 __global__ void pack_kernel(nz_walkers wk, const uint32_t* ids, nz_state st);
 __global__ void disp_moments_kernel(const float* __restrict__ disp, int N, double* __restrict__ out);
 __global__ void unpack_kernel(nz_state st, nz_walkers wk, int by_id, int* bad);

@@ -46,21 +46,41 @@ struct ScanOut {
   bool any_in;
 };
 
+// One list entry: its sphere's record and a key.  Record lists (LK 0): the
+// record inline, the key the structure id (-1 for a walker in the box, which
+// reads none).  Index lists (LK 2 or 4): the key the record index, the record
+// read from the substrate's record array.
+template <int LK>
+__device__ __forceinline__ void entry(const void* __restrict__ list, const float4* __restrict__ rec,
+                                      const int* __restrict__ sid, int k, bool box, int& key, float4& c) {
+  if constexpr (LK == 0) {
+    key = box ? -1 : __ldg(sid + k);
+    c = __ldg(rec + k);
+  } else {
+    if constexpr (LK == 2) key = int(__ldg(static_cast<const unsigned short*>(list) + k));
+    else key = __ldg(static_cast<const int*>(list) + k);
+    c = __ldg(rec + key);
+  }
+}
+
 // One pass over a cell's list under assumed label L.  Returns false when the
 // walker's label is not L (then nothing in `o` is used).  The entries of a
 // cell are ordered by structure id: the pass ends at the first entry of a
-// structure above L (the reference skips those spheres, :805-806).  Entries
-// are read kScanBatch at a time (1 measured fastest on the packed workload).
-template <bool T64>
-__device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const int* __restrict__ sid, int start,
-                                          int count, int nstructures, float x, float y, float z, int L, float a,
-                                          float jx, float jy, float jz, float reach, ScanOut& o) {
+// structure above L (the reference skips those spheres, :805-806).  In index
+// form an entry's structure is compared through its record index: records
+// [lo, hi) are structure L's, so key < hi is "structure <= L" and key < lo
+// "structure < L".
+template <int LK, bool T64>
+__device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const float4* __restrict__ rec,
+                                          const int* __restrict__ sid, int start, int count, int nstructures,
+                                          int lo, int hi, float x, float y, float z, int L, float a, float jx,
+                                          float jy, float jz, float reach, ScanOut& o) {
   o.fin = 0.0f;
   o.fout = kBig;
   o.any_in = false;
   bool found = false, lower = false, stop = false;
   // A walker in the box (label nstructures) has every entry below its label:
-  // nothing to stop at and no structure id to read.
+  // nothing to stop at and no structure to compare.
   const bool box = L >= nstructures;
   const float slack = kTol + reach * 1.02f + 2e-3f;
   for (int base = 0; base < count && !stop; base += 32) {
@@ -70,46 +90,34 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
     // sphere neither contains the walker nor lies within this iteration's
     // reach; predicated, one entry per load
     uint32_t near_mask = 0u;
-    for (int i0 = 0; i0 < m && !stop; i0 += kScanBatch) {
-      int sv[kScanBatch];
-      float4 cv[kScanBatch];
-#pragma unroll
-      for (int u = 0; u < kScanBatch; ++u) {
-        const int k = start + base + i0 + u;
-        if (i0 + u < m) {
-          sv[u] = box ? -1 : __ldg(sid + k);
-          cv[u] = __ldg(sph4 + k);
-        } else {
-          sv[u] = 0x7fffffff;
-          cv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kScanBatch; ++u) {
-        const bool valid = sv[u] <= L;
-        stop |= !valid;
-        const float dx = x - cv[u].x, dy = y - cv[u].y, dz = z - cv[u].z;
-        // a filter, not the reference's arithmetic: fused multiply-adds are
-        // fine here (their rounding is far inside the slack)
-        const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
-        const float t = cv[u].w + slack;
-        near_mask |= (valid && d2 <= t * t) ? (1u << (i0 + u)) : 0u;
-      }
+    for (int i = 0; i < m && !stop; ++i) {
+      int key;
+      float4 c;
+      entry<LK>(list, rec, sid, start + base + i, box, key, c);
+      const bool valid = LK == 0 ? key <= L : (box || key < hi);
+      stop |= !valid;
+      const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
+      // a filter, not the reference's arithmetic: fused multiply-adds are
+      // fine here (their rounding is far inside the slack)
+      const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+      const float t = c.w + slack;
+      near_mask |= (valid && d2 <= t * t) ? (1u << i) : 0u;
     }
     // second pass, near entries only: the reference's inside test, then the
     // fraction of a containing sphere or of a lower structure's sphere
     while (near_mask) {
       const int i = __ffs(near_mask) - 1;
       near_mask &= near_mask - 1;
-      const int k = start + base + i;
-      const float4 c = __ldg(sph4 + k);
-      const int s = box ? -1 : __ldg(sid + k);
+      int key;
+      float4 c;
+      entry<LK>(list, rec, sid, start + base + i, box, key, c);
+      const bool below = LK == 0 ? key < L : (box || key < lo);
       const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
       const float d2 = dx * dx + dy * dy + dz * dz;
       const bool inside = d2 - c.w * c.w < 0;
-      lower |= inside && (s < L);
-      found |= inside && (s >= L);
-      if (inside || s < L) {
+      lower |= inside && below;
+      found |= inside && !below;
+      if (inside || below) {
         const float f = step_either_t<T64>(inside, dx, dy, dz, c.w, a, jx, jy, jz);
         if (inside) {
           o.any_in = true;
@@ -124,18 +132,38 @@ __device__ __forceinline__ bool scan_cell(const float4* __restrict__ sph4, const
 }
 
 // The reference's label pass (sim3d_kernel.cu:766-785): lowest structure id
-// among the spheres containing the walker, nstructures if none.
-__device__ __forceinline__ int label_of(const float4* __restrict__ sph4, const int* __restrict__ sid, int start,
+// among the spheres containing the walker, nstructures if none.  In index
+// form the entries ascend by structure, so the first containing one decides.
+template <int LK>
+__device__ __forceinline__ int label_of(const void* __restrict__ list, const float4* __restrict__ rec,
+                                        const int* __restrict__ sid, const int* __restrict__ rec_sid, int start,
                                         int count, int nstructures, float x, float y, float z) {
   int L = nstructures;
   for (int i = 0; i < count; ++i) {
-    const int s = __ldg(sid + start + i);
-    if (s < L) {
-      const float4 c = __ldg(sph4 + start + i);
-      if (inside_test(x - c.x, y - c.y, z - c.z, c.w) < 0) L = s;
+    if constexpr (LK == 0) {
+      const int s = __ldg(sid + start + i);
+      if (s < L) {
+        const float4 c = __ldg(rec + start + i);
+        if (inside_test(x - c.x, y - c.y, z - c.z, c.w) < 0) L = s;
+      }
+    } else {
+      int key;
+      float4 c;
+      entry<LK>(list, rec, sid, start + i, false, key, c);
+      if (inside_test(x - c.x, y - c.y, z - c.z, c.w) < 0) return __ldg(rec_sid + key);
     }
   }
   return L;
+}
+
+// Records [lo, hi) of structure L in index form (hi = lo = S for the box).
+__device__ __forceinline__ void label_bounds(const JobDev& J, int L, int& lo, int& hi) {
+  if (L >= J.nstructures) {
+    lo = hi = J.S;
+  } else {
+    lo = __ldg(J.sid_start + L);
+    hi = __ldg(J.sid_start + L + 1);
+  }
 }
 
 // Cell of the walker at the start of a step and the cell's low corner.
@@ -163,7 +191,7 @@ __device__ __forceinline__ void jump_of(const JobDev& J, uint32_t wid, int s, in
 // compensation and the step's jump; the origin (spins0) and the flag word stay
 // in memory and are updated in place on the rare wrap / iteration-cap events
 // (except with moments, which read the origin every step).
-template <int MODE>
+template <int MODE, int LK>
 __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1, double* s_mom) {
   constexpr bool kMom = (MODE & NZ_MODE_MOMENTS) != 0;
   constexpr bool kDisp = (MODE & kModeDisp) != 0;
@@ -187,9 +215,11 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     x0 = O.x; y0 = O.y; z0 = O.z;
   }
   if (label < 0 || label > J.nstructures) label = J.nstructures;
+  int lo = 0, hi = 0;  // index form: structure `label`'s records
+  if (LK) label_bounds(J, label, lo, hi);
 
   const float dt = J.dt;
-  const bool has_near = J.near_sph4 != nullptr;
+  const bool has_near = (LK ? J.near_idx : static_cast<const void*>(J.near_sph4)) != nullptr;
   int s = s0;
   int niter = 0, draw = 0, cell = 0;
   // start and count of the step cell's primary list (the near list where
@@ -225,8 +255,9 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
       const float dist = sqrtf(ex * ex + ey * ey + ez * ez);
       near = (dist + reach) * 1.02f + kTol + 2e-3f <= J.near_margin;
     }
-    const float4* sph4 = near ? J.near_sph4 : J.sph4;
-    const int* sidv = near ? J.near_sid : J.sid;
+    const void* list = LK ? (near ? J.near_idx : J.idx) : nullptr;
+    const float4* sph4 = LK ? J.rec4 : (near ? J.near_sph4 : J.sph4);
+    const int* sidv = LK ? nullptr : (near ? J.near_sid : J.sid);
     int start = pstart, count = pcount;
     if (has_near && !near) {
       start = __ldg(J.cell_start + cell);
@@ -234,8 +265,10 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     }
     ScanOut r;
     constexpr bool kT64 = (MODE & NZ_MODE_TANGENT64) != 0;
-    if (!scan_cell<kT64>(sph4, sidv, start, count, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r)) {
-      label = label_of(sph4, sidv, start, count, J.nstructures, x, y, z);
+    if (!scan_cell<LK, kT64>(list, sph4, sidv, start, count, J.nstructures, lo, hi, x, y, z, label, a, jx, jy, jz,
+                             reach, r)) {
+      label = label_of<LK>(list, sph4, sidv, J.rec_sid, start, count, J.nstructures, x, y, z);
+      if (LK) label_bounds(J, label, lo, hi);
       if (niter == 1) {  // the first draw's length depends on the label
         ds = sqrtf(2 * __ldg(J.D + label) * dt);
         ds_label = label;
@@ -245,7 +278,8 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
       }
       // the full list: the near one was chosen for the old reach
       const int fs = __ldg(J.cell_start + cell), fc = __ldg(J.cell_count + cell);
-      scan_cell<kT64>(J.sph4, J.sid, fs, fc, J.nstructures, x, y, z, label, a, jx, jy, jz, reach, r);
+      scan_cell<LK, kT64>(LK ? J.idx : nullptr, LK ? J.rec4 : J.sph4, LK ? nullptr : J.sid, fs, fc, J.nstructures, lo,
+                          hi, x, y, z, label, a, jx, jy, jz, reach, r);
     }
     jc = ref_min(jc, r.any_in ? r.fin : kBig);
     jc = ref_min(jc, r.fout);
@@ -351,14 +385,14 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
 
 // One work item: walkers [first, first + count) of job J, steps [step0, step1)
 // clamped to the job's protocol.
-template <int MODE>
+template <int MODE, int LK>
 __device__ __forceinline__ void run_item(const JobDev& J, int first, int count, int step0, int step1, double* s_mom) {
   const int s0 = step0 + J.step_offset, s1 = min(step1 + J.step_offset, J.nsteps);
   if (MODE & NZ_MODE_MOMENTS) {
     for (int i = threadIdx.x; i < kMomentSteps * 6; i += blockDim.x) s_mom[i] = 0.0;
     __syncthreads();
   }
-  if (threadIdx.x < count && s0 < s1) walk_one<MODE>(J, first + threadIdx.x, s0, s1, s_mom);
+  if (threadIdx.x < count && s0 < s1) walk_one<MODE, LK>(J, first + threadIdx.x, s0, s1, s_mom);
   if (MODE & NZ_MODE_MOMENTS) {
     __syncthreads();
     if (J.moments)
@@ -372,7 +406,7 @@ __device__ __forceinline__ void run_item(const JobDev& J, int first, int count, 
 // value, item i = walkers [i*T, i*T + T).  Otherwise jobs and items come from
 // device arrays; with queue != null the grid is persistent and each CTA takes
 // items from *queue until none is left.
-template <int MODE, bool SINGLE>
+template <int MODE, int LK, bool SINGLE>
 __global__ void __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
     walk_fused_kernel(const __grid_constant__ JobDev single, const nz_job* __restrict__ jobs,
                       const nz_item* __restrict__ items, int n_items, int step0, int step1, int* queue) {
@@ -391,7 +425,7 @@ __global__ void __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
     if (SINGLE) {
       const int first = it * int(blockDim.x);
       const int count = min(int(blockDim.x), single.nwalkers - first);
-      run_item<MODE>(single, first, count, step0, step1, s_mom);
+      run_item<MODE, LK>(single, first, count, step0, step1, s_mom);
     } else {
       // every thread of the CTA works on the same job: its descriptor lives
       // in shared memory, not in each thread's registers
@@ -402,7 +436,7 @@ __global__ void __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
         s_job.step_offset = a.step_offset;
       }
       __syncthreads();
-      run_item<MODE>(s_job, wi.first, wi.count, step0, step1, s_mom);
+      run_item<MODE, LK>(s_job, wi.first, wi.count, step0, step1, s_mom);
       __syncthreads();
     }
     if (!queue) return;
@@ -477,6 +511,12 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
   j.near_count = sub.near_count;
   j.near_sph4 = reinterpret_cast<const float4*>(sub.near_sph4);
   j.near_sid = sub.near_sid;
+  j.idx = sub.idx_bytes ? sub.cell_idx : nullptr;
+  j.near_idx = sub.idx_bytes ? sub.near_idx : nullptr;
+  j.rec4 = reinterpret_cast<const float4*>(sub.rec4);
+  j.rec_sid = sub.rec_sid;
+  j.sid_start = sub.sid_start;
+  j.S = sub.S;
   j.D = sub.D;
   j.T2 = sub.T2;
   j.G = G;
@@ -496,7 +536,7 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
   return j;
 }
 
-template <int MODE>
+template <int MODE, int LK>
 void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0, int step1,
                  int* queue, int grid, int threads, cudaStream_t st) {
   // the kernel keeps little in shared memory: prefer the whole carveout for
@@ -506,59 +546,74 @@ void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items,
   if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) {
     static std::once_flag once[kMaxDevices];
     std::call_once(once[dev], [] {
-      cudaFuncSetAttribute(walk_fused_kernel<MODE, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-      cudaFuncSetAttribute(walk_fused_kernel<MODE, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+      cudaFuncSetAttribute(walk_fused_kernel<MODE, LK, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+      cudaFuncSetAttribute(walk_fused_kernel<MODE, LK, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     });
   }
   if (jobs)
-    walk_fused_kernel<MODE, false><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
+    walk_fused_kernel<MODE, LK, false><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
   else
-    walk_fused_kernel<MODE, true><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
+    walk_fused_kernel<MODE, LK, true><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
 }
 
-// jobs == null: the single job `single` with n_items CTAs of kFusedThreads walkers.
-int launch_fused(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
-                 int step1, int* queue, int grid, int threads, cudaStream_t st) {
+template <int LK>
+int launch_lk(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
+              int step1, int* queue, int grid, int threads, cudaStream_t st) {
+#define NZ_LAUNCH(M) launch_mode<(M), LK>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st)
   switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS | NZ_MODE_TANGENT64 | kModeDisp)) {
-    case NZ_MODE_PHI | NZ_MODE_TANGENT64:
-      launch_mode<NZ_MODE_PHI | NZ_MODE_TANGENT64>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
-      break;
-    case NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_TANGENT64:
-      launch_mode<NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_TANGENT64>(single, jobs, items, n_items, step0, step1, queue, grid,
-                                                                 threads, st);
-      break;
-    case NZ_MODE_PHI: launch_mode<NZ_MODE_PHI>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
-    case NZ_MODE_SIG: launch_mode<NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
-    case NZ_MODE_PHI | NZ_MODE_SIG:
-      launch_mode<NZ_MODE_PHI | NZ_MODE_SIG>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
-    case NZ_MODE_SIG | NZ_MODE_MOMENTS:
-      launch_mode<NZ_MODE_SIG | NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
-    case NZ_MODE_MOMENTS:
-      launch_mode<NZ_MODE_MOMENTS>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
-    case NZ_MODE_SIG | kModeDisp:
-      launch_mode<NZ_MODE_SIG | kModeDisp>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
-    case kModeDisp:
-      launch_mode<kModeDisp>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
-    case 0: launch_mode<0>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st); break;
+    case NZ_MODE_PHI | NZ_MODE_TANGENT64: NZ_LAUNCH(NZ_MODE_PHI | NZ_MODE_TANGENT64); break;
+    case NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_TANGENT64: NZ_LAUNCH(NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_TANGENT64); break;
+    case NZ_MODE_PHI: NZ_LAUNCH(NZ_MODE_PHI); break;
+    case NZ_MODE_SIG: NZ_LAUNCH(NZ_MODE_SIG); break;
+    case NZ_MODE_PHI | NZ_MODE_SIG: NZ_LAUNCH(NZ_MODE_PHI | NZ_MODE_SIG); break;
+    case NZ_MODE_SIG | NZ_MODE_MOMENTS: NZ_LAUNCH(NZ_MODE_SIG | NZ_MODE_MOMENTS); break;
+    case NZ_MODE_MOMENTS: NZ_LAUNCH(NZ_MODE_MOMENTS); break;
+    case NZ_MODE_SIG | kModeDisp: NZ_LAUNCH(NZ_MODE_SIG | kModeDisp); break;
+    case kModeDisp: NZ_LAUNCH(kModeDisp); break;
+    case 0: NZ_LAUNCH(0); break;
     default: return set_error(NZ_ERR_ARG, "fused walk: unsupported mode %d", mode);
   }
+#undef NZ_LAUNCH
   return check_launch("walk_fused_kernel");
 }
 
-int occupancy_fused(int mode, int threads, int* blocks_per_sm) {
-  cudaError_t e;
+// jobs == null: the single job `single` with n_items CTAs of kFusedThreads walkers.
+int launch_fused(int mode, int lk, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items,
+                 int step0, int step1, int* queue, int grid, int threads, cudaStream_t st) {
+  switch (lk) {
+    case 0: return launch_lk<0>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
+    case 2: return launch_lk<2>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
+    case 4: return launch_lk<4>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
+    default: return set_error(NZ_ERR_ARG, "fused walk: list kind %d is not 0, 2 or 4", lk);
+  }
+}
+
+template <int LK>
+cudaError_t occupancy_lk(int mode, int threads, int* blocks_per_sm) {
   switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS)) {
     case NZ_MODE_PHI:
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<NZ_MODE_PHI, false>, threads, 0);
-      break;
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<NZ_MODE_PHI, LK, false>,
+                                                           threads, 0);
     case NZ_MODE_SIG:
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<NZ_MODE_SIG, false>, threads, 0);
-      break;
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<NZ_MODE_SIG, LK, false>,
+                                                           threads, 0);
     case NZ_MODE_PHI | NZ_MODE_SIG:
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm,
-                                                         walk_fused_kernel<NZ_MODE_PHI | NZ_MODE_SIG, false>, threads, 0);
-      break;
-    default: return set_error(NZ_ERR_ARG, "occupancy: unsupported batch mode %d", mode);
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          blocks_per_sm, walk_fused_kernel<NZ_MODE_PHI | NZ_MODE_SIG, LK, false>, threads, 0);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int occupancy_fused(int mode, int lk, int threads, int* blocks_per_sm) {
+  const int m = mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS);
+  if (m != NZ_MODE_PHI && m != NZ_MODE_SIG && m != (NZ_MODE_PHI | NZ_MODE_SIG))
+    return set_error(NZ_ERR_ARG, "occupancy: unsupported batch mode %d", mode);
+  cudaError_t e;
+  switch (lk) {
+    case 0: e = occupancy_lk<0>(mode, threads, blocks_per_sm); break;
+    case 2: e = occupancy_lk<2>(mode, threads, blocks_per_sm); break;
+    case 4: e = occupancy_lk<4>(mode, threads, blocks_per_sm); break;
+    default: return set_error(NZ_ERR_ARG, "occupancy: list kind %d is not 0, 2 or 4", lk);
   }
   if (e != cudaSuccess) return set_error(NZ_ERR_CUDA, "occupancy: %s", cudaGetErrorString(e));
   return NZ_OK;

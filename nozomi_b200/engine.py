@@ -79,15 +79,26 @@ def box_grid(L3, nseg) -> L.Grid:
 class DeviceSubstrate:
     """Spheres [5,S] (cx, cy, cz, r, structure id), box, cell grid, compact cell
     lists built on the GPU (DiffSim3d.set_segments, diffsim3d.py:107-174), the
-    per-entry sphere records of the fused walk, and D / T2 per structure."""
+    fused walk's form of those lists, and D / T2 per structure.
+
+    idx_bytes selects the fused walk's list form: 0, per-entry records (each
+    entry carries its sphere's centre, radius and structure id); 2 or 4, index
+    lists (each entry a 16- or 32-bit index into one record array of the
+    substrate, the spheres sorted by structure id); None, index lists of 16
+    bits when S <= 65536, else 32."""
 
     def __init__(self, spheres: np.ndarray, nstructures: int, L3, nseg, D, T2, jump_tol: float = 1.0,
-                 cells: tuple | None = None, near_margin: float | None = None):
+                 cells: tuple | None = None, near_margin: float | None = None, idx_bytes: int | None = None):
         sph64 = np.ascontiguousarray(spheres, dtype=np.float64).reshape(5, -1)
         validate_substrate(sph64, int(nstructures), L3, nseg, D, T2)
         require_cuda()
         dev = _dev()
         self.S = sph64.shape[1]
+        if idx_bytes is None:
+            idx_bytes = 2 if self.S <= 65536 else 4
+        if idx_bytes not in (0, 2, 4) or (idx_bytes == 2 and self.S > 65536):
+            raise NozomiError(f"list form idx_bytes={idx_bytes} does not suit {self.S} spheres (0, 2 up to 65536, 4)")
+        self.idx_bytes = int(idx_bytes)
         self.nstructures = int(nstructures)
         self.L = tuple(float(v) for v in L3)
         self.nseg = tuple(int(v) for v in nseg)
@@ -106,11 +117,37 @@ class DeviceSubstrate:
             self.cell_count = torch.as_tensor(np.asarray(ct, np.int32), device=dev)
             self.cell_items = torch.as_tensor(np.asarray(it, np.int32), device=dev)
             self.n_items = int(self.cell_items.numel())
+        if self.idx_bytes:
+            self._records(sph64)
         self._gather()
         self.near_margin = None
         self.near = None
         if near_margin is not None:
             self.set_near_margin(near_margin)
+
+    def _records(self, sph64: np.ndarray):
+        """The index form's record array: spheres sorted by structure id
+        (stable), their records and ids, the first record of every structure,
+        and each sphere's record index (perm)."""
+        dev = _dev()
+        sid = sph64[4].astype(np.int64)
+        order = np.argsort(sid, kind="stable")
+        perm = np.empty(self.S, np.int32)
+        perm[order] = np.arange(self.S, dtype=np.int32)
+        rec_sid = sid[order].astype(np.int32)
+        self.rec4 = torch.from_numpy(np.ascontiguousarray(sph64[:4, order].T.astype(np.float32))).to(dev)
+        self.rec_sid = torch.from_numpy(rec_sid).to(dev)
+        self.sid_start = torch.from_numpy(
+            np.searchsorted(rec_sid, np.arange(self.nstructures + 2)).astype(np.int32)).to(dev)
+        self.perm = torch.from_numpy(perm).to(dev)
+
+    def _index(self, start, count, items, n):
+        """Index-form entries of member lists (start, count, items)."""
+        dt = torch.int16 if self.idx_bytes == 2 else torch.int32
+        idx = torch.empty(max(n, 1), dtype=dt, device=_dev())
+        L.check(L.load().nz_cells_index(_p(items), n, _p(self.perm), self.S, _p(start), _p(count), self.ncell, _p(idx),
+                                        self.idx_bytes, _stream()), "nz_cells_index")
+        return idx
 
     def _build_cells(self, margin: float | None = None, store: bool = True):
         dev = _dev()
@@ -146,16 +183,27 @@ class DeviceSubstrate:
             raise NozomiError(f"near margin {margin} must lie in (0, {self.jump_tol})")
         st, ct, it, n = self._build_cells(margin, store=False)
         dev = _dev()
+        if self.idx_bytes:
+            self.near_margin = margin
+            self.near = (st, ct, it, None, None, self._index(st, ct, it, n))
+            return
         sph4 = torch.empty((max(n, 1), 4), dtype=torch.float32, device=dev)
         sid = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
         L.check(L.load().nz_cells_gather(_p(self.spheres), self.S, _p(it), n, _p(st), _p(ct), self.ncell, _p(sph4),
                                          _p(sid), _stream()), "nz_cells_gather")
         self.near_margin = margin
-        self.near = (st, ct, it, sph4, sid)
+        self.near = (st, ct, it, sph4, sid, None)
 
     def _gather(self):
+        """The fused walk's form of the member lists: index entries, or
+        per-entry records."""
         dev = _dev()
         n = int(self.n_items)
+        if self.idx_bytes:
+            self.cell_sph4 = self.cell_sid = None
+            self.cell_idx = self._index(self.cell_start, self.cell_count, self.cell_items, n)
+            return
+        self.cell_idx = None
         self.cell_sph4 = torch.empty((max(n, 1), 4), dtype=torch.float32, device=dev)
         self.cell_sid = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
         L.check(L.load().nz_cells_gather(_p(self.spheres), self.S, _p(self.cell_items), n, _p(self.cell_start),
@@ -185,26 +233,32 @@ class DeviceSubstrate:
         other.cell_count = torch.full((self.ncell,), K, dtype=torch.int32, device=dev)
         other.cell_items = seg
         other.n_items = int(seg.numel())
-        other._gather()
+        other._gather()  # in the index form the record array (and perm) is shared
         other.K = K
         other.near_margin, other.near = None, None
         return other
 
     def struct(self) -> L.Substrate:
+        ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
         s = L.Substrate(self.grid, self.nstructures, self.S, self.spheres.data_ptr(), self.cell_start.data_ptr(),
-                        self.cell_count.data_ptr(), self.cell_items.data_ptr(), self.cell_sph4.data_ptr(),
-                        self.cell_sid.data_ptr(), self.D.data_ptr(), self.T2.data_ptr())
+                        self.cell_count.data_ptr(), self.cell_items.data_ptr(), ptr(self.cell_sph4),
+                        ptr(self.cell_sid), self.D.data_ptr(), self.T2.data_ptr())
         if self.near is not None:
-            st, ct, _, sph4, sid = self.near
+            st, ct, _, sph4, sid, nidx = self.near
             s.near_margin = self.near_margin
             s.near_start, s.near_count = st.data_ptr(), ct.data_ptr()
-            s.near_sph4, s.near_sid = sph4.data_ptr(), sid.data_ptr()
+            s.near_sph4, s.near_sid, s.near_idx = ptr(sph4), ptr(sid), ptr(nidx)
+        if self.idx_bytes:
+            s.idx_bytes, s.cell_idx = self.idx_bytes, self.cell_idx.data_ptr()
+            s.rec4, s.rec_sid, s.sid_start = self.rec4.data_ptr(), self.rec_sid.data_ptr(), self.sid_start.data_ptr()
         return s
 
     def nbytes(self) -> int:
         ts = [self.spheres64, self.spheres, self.D, self.T2, self.cell_start, self.cell_count, self.cell_items,
-              self.cell_sph4, self.cell_sid] + (list(self.near) if self.near is not None else [])
-        return sum(t.numel() * t.element_size() for t in ts)
+              self.cell_sph4, self.cell_sid, self.cell_idx] + (list(self.near) if self.near is not None else [])
+        if self.idx_bytes:
+            ts += [self.rec4, self.rec_sid, self.sid_start, self.perm]
+        return sum(t.numel() * t.element_size() for t in ts if t is not None)
 
 
 def philox_draws(key: int, stream_id: int = 0) -> L.Draws:

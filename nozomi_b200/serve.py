@@ -50,7 +50,7 @@ import torch
 
 from . import engine
 from . import _lib as L
-from .batch import JobSpec, SubstrateCache, _job_table, _items, _sort_table
+from .batch import LIST_BITS, JobSpec, SubstrateCache, _job_table, _items, _sort_table, batch_grid, list_groups
 from .simulate import Tuning
 from .substrates import cell_grid
 from .waveforms import step_tables
@@ -114,11 +114,8 @@ class Server:
         self.dev = dev
         self.compute = torch.cuda.current_stream(dev)
         self.side = torch.cuda.Stream(dev)
-        sms = torch.cuda.get_device_properties(dev).multi_processor_count
-        occ = ctypes.c_int(0)
-        L.check(L.load().nz_batch_occupancy(L.MODE_PHI, threads, ctypes.byref(occ)), "nz_batch_occupancy")
-        self.grid = sms * max(1, occ.value)
-        self.queue = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.grids = {lk: batch_grid(threads, lk) for lk in (0, 2, 4)}
+        self.queue = torch.zeros(3, dtype=torch.int32, device=dev)
         self.sort_scratch = torch.empty(1, dtype=torch.uint8, device=dev)
         self.clock = time.perf_counter
         self.on_wait = None  # called while a round runs (the request loop submits arrivals there)
@@ -247,17 +244,21 @@ class Server:
             if self.sort_scratch.numel() < need:
                 self.sort_scratch = torch.empty(need, dtype=torch.uint8, device=self.dev)
             table = _job_table(jobs, [j["buf"][j["cur"]] for j in jobs])
-            items = _items(self._as_plan(jobs), list(range(len(jobs))), self.threads, 0, k)
+            plan = self._as_plan(jobs)
+            groups = [(lk, _items(plan, grp, self.threads, 0, k))
+                      for lk, grp in sorted(list_groups(jobs, range(len(jobs))).items())]
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(self.compute)
             L.check(lib.nz_batch_sort(ctypes.c_void_p(sort.data_ptr()), n_sort, tw, tk,
                                       ctypes.c_void_p(self.sort_scratch.data_ptr()), self.sort_scratch.numel(),
                                       stream), "nz_batch_sort")
             self.queue.zero_()
-            L.check(lib.nz_walk_batch(ctypes.c_void_p(table.data_ptr()), len(jobs),
-                                      ctypes.c_void_p(items.data_ptr()), int(items.shape[0]), L.MODE_PHI, 0, k,
-                                      ctypes.c_void_p(self.queue.data_ptr()), self.grid, self.threads, stream),
-                    "nz_walk_batch")
+            for g, (lk, items) in enumerate(groups):
+                L.check(lib.nz_walk_batch(ctypes.c_void_p(table.data_ptr()), len(jobs),
+                                          ctypes.c_void_p(items.data_ptr()), int(items.shape[0]),
+                                          L.MODE_PHI | LIST_BITS[lk], 0, k,
+                                          ctypes.c_void_p(self.queue.data_ptr() + 4 * g), self.grids[lk],
+                                          self.threads, stream), "nz_walk_batch")
             e1.record(self.compute)
             finished, ws = [], 0
             for t in self.active:

@@ -29,17 +29,29 @@ class Tuning:
     coarsen: int = 4              # re-binning bins = cells coarsened by this factor per axis
     by_label: bool = True         # re-bin by (label, bin): a warp's walkers share a structure
     near_margin: float | None = 0.5  # margin of the near lists (None: full lists only)
+    lists: str = "index"          # the fused walk's list form: "index" (16/32-bit) or "records"
+
+
+def idx_bytes_for(lists: str):
+    """DeviceSubstrate's idx_bytes for a Tuning.lists value."""
+    if lists == "records":
+        return 0
+    if lists == "index":
+        return None
+    raise ValueError(f"list form {lists!r} is not 'index' or 'records'")
 
 
 def device_substrate(sub: Substrate, D=2.0, T2=100.0, cell: float = 1.0, nseg=None, D_box=None,
-                     jump_tol: float = 1.0, near_margin: float | None = None) -> engine.DeviceSubstrate:
+                     jump_tol: float = 1.0, near_margin: float | None = None,
+                     lists: str = "index") -> engine.DeviceSubstrate:
     nseg = cell_grid(sub.L, cell) if nseg is None else nseg
     ns = sub.nstructures
     Dv = np.full(ns + 1, D, np.float32)
     if D_box is not None:
         Dv[ns] = D_box
     T2v = np.full(ns + 1, T2, np.float32)
-    return engine.DeviceSubstrate(sub.spheres(), ns, sub.L, nseg, Dv, T2v, jump_tol=jump_tol, near_margin=near_margin)
+    return engine.DeviceSubstrate(sub.spheres(), ns, sub.L, nseg, Dv, T2v, jump_tol=jump_tol, near_margin=near_margin,
+                                  idx_bytes=idx_bytes_for(lists))
 
 
 class DwiRun:
@@ -163,6 +175,6 @@ def simulate_dwi(sub: Substrate, gwave, dirs, bvalues=None, amplitudes=None, N: 
     if amplitudes is None:
         amplitudes = gwave.amplitude_for_b(bvalues)
     tuning = tuning or Tuning()
-    dsub = device_substrate(sub, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin)
+    dsub = device_substrate(sub, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin, lists=tuning.lists)
     run = DwiRun(dsub, gwave, dirs, amplitudes, N, seed=seed, targets=targets, tuning=tuning).prepare()
     return run.walk().signal()

@@ -186,6 +186,32 @@ def test_invalid_arguments_rejected_without_gpu():
     near = _fused_substrate(_lib)
     near.near_sph4, near.near_margin = FAKE, 0.5  # near records without their index arrays
     refused(lib.nz_walk_fused(by(near), by(a), 0, 0.01, None, None, 0, 10, by(draws), None, None), "nz_walk_fused")
+    # index lists: a width other than 2 or 4, 16 bits for too many spheres, a
+    # missing record array, misaligned records, near entries without offsets
+    ix = _fused_substrate(_lib)
+    ix.cell_sph4 = ix.cell_sid = None
+    ix.idx_bytes, ix.cell_idx, ix.rec4, ix.rec_sid, ix.sid_start = 2, FAKE, FAKE, FAKE, FAKE
+    for field, value in (("idx_bytes", 3), ("S", 70000), ("rec4", None), ("rec4", FAKE + 8), ("sid_start", None),
+                         ("near_idx", FAKE)):
+        bad = _fused_substrate(_lib)
+        ctypes.pointer(bad)[0] = ix
+        setattr(bad, field, value)
+        refused(lib.nz_walk_fused(by(bad), by(a), 0, 0.01, None, None, 0, 10, by(draws), None, None),
+                "nz_walk_fused")
+    assert lib.nz_walk_fused(by(ix), by(empty_state := _lib.State(0, None, None, None, None)), 0, 0.01, None, None,
+                             0, 10, by(draws), None, None) == 0
+    ix.S = 70000
+    ix.idx_bytes = 4  # 32-bit entries take any sphere count
+    assert lib.nz_walk_fused(by(ix), by(empty_state), 0, 0.01, None, None, 0, 10, by(draws), None, None) == 0
+    refused(lib.nz_cells_index(FAKE, 10, None, 70000, FAKE, FAKE, 8, FAKE, 2, None), "nz_cells_index")
+    refused(lib.nz_cells_index(FAKE, 10, None, 100, FAKE, FAKE, 8, FAKE, 3, None), "nz_cells_index")
+    refused(lib.nz_cells_index(FAKE, 10, None, 100, FAKE, FAKE, 0, FAKE, 2, None), "nz_cells_index")
+    assert lib.nz_cells_index(None, 0, None, 100, None, None, 8, None, 2, None) == 0
+    refused(lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_PHI | _lib.LIST_IDX16 | _lib.LIST_IDX32, 0, 100, FAKE, 148,
+                              128, None), "nz_walk_batch")
+    occ = ctypes.c_int(0)
+    refused(lib.nz_batch_occupancy(_lib.MODE_PHI | _lib.LIST_IDX16 | _lib.LIST_IDX32, 128, ctypes.byref(occ)),
+            "nz_batch_occupancy")
     # moments walk: scratch below [steps][3][N] floats, or an unsupported mode
     small = lib.nz_walk_fused_moments_scratch_bytes(N, 100) - 4
     refused(lib.nz_walk_fused_moments(by(sub), by(a), 0, 0.01, None, None, 0, 100, by(draws), FAKE, small, FAKE,

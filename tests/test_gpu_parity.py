@@ -31,7 +31,7 @@ def _dev(a, dtype=None):
     return t.cuda()
 
 
-def _sub_from_case(eng, c, padded=True):
+def _sub_from_case(eng, c, padded=True, idx_bytes=None):
     nseg = tuple(int(v) for v in c["nseg"])
     if padded:
         from oracle.cells_oracle import padded_as_lists
@@ -39,7 +39,12 @@ def _sub_from_case(eng, c, padded=True):
         cells = padded_as_lists(int(c["K"]), c["segments"], ncell)
     else:
         cells = None
-    return eng.DeviceSubstrate(c["spheres"], int(c["nstructures"]), tuple(c["L"]), nseg, c["D"], c["T2"], cells=cells)
+    return eng.DeviceSubstrate(c["spheres"], int(c["nstructures"]), tuple(c["L"]), nseg, c["D"], c["T2"], cells=cells,
+                               idx_bytes=idx_bytes)
+
+
+# the fused walk's list forms: per-entry records, 16-bit and 32-bit index lists
+LIST_FORMS = [0, 2, 4]
 
 
 def test_cells_match_oracle(eng):
@@ -114,13 +119,14 @@ def test_plain_dwi_matches_reference(eng, name):
     np.testing.assert_array_equal(wk.phase.cpu().numpy(), c["phase"])
 
 
+@pytest.mark.parametrize("idx_bytes", LIST_FORMS)
 @pytest.mark.parametrize("name", DWI + EDGE + NARROW[:2])
-def test_fused_matches_oracle_and_reference(eng, name):
+def test_fused_matches_oracle_and_reference(eng, name, idx_bytes):
     """The fused kernel (one launch for all steps, Phi form) against the oracle
     with the same cell lists: positions, spins0, labels and Phi bit-exact; and
-    positions against the reference's own outputs."""
+    positions against the reference's own outputs.  In every list form."""
     c = load(name)
-    sub = _sub_from_case(eng, c)
+    sub = _sub_from_case(eng, c, idx_bytes=idx_bytes)
     N = int(c["N"])
     nt = int(c["nt"])
     dt = float(c["dt"])
@@ -274,15 +280,17 @@ def test_signal_and_moments_match_oracle(eng):
     np.testing.assert_allclose(m.cpu().numpy(), oz.moments(x.cpu().numpy(), s0), rtol=1e-10)
 
 
+@pytest.mark.parametrize("idx_bytes", [0, 2])
 @pytest.mark.parametrize("name,margin", [("dwi_c1_cells", 0.5), ("dwi_c1_cells", 0.25), ("dwi_overlap", 0.4),
                                          ("narrow_periodic_in", 0.3), ("dwi_faces", 0.3), ("dwi_faces", 0.6)])
-def test_fused_near_lists_match_full_lists(eng, name, margin):
+def test_fused_near_lists_match_full_lists(eng, name, margin, idx_bytes):
     """Near lists (smaller margin, used when an iteration's reach fits) give
     the full lists' result bit for bit: the fused walk with near lists against
-    the oracle on the full member lists."""
+    the oracle on the full member lists, records and 16-bit index form."""
     c = load(name)
     sph, L3, nseg = c["spheres"], tuple(c["L"]), tuple(int(v) for v in c["nseg"])
-    sub = eng.DeviceSubstrate(sph, int(c["nstructures"]), L3, nseg, c["D"], c["T2"], near_margin=margin)
+    sub = eng.DeviceSubstrate(sph, int(c["nstructures"]), L3, nseg, c["D"], c["T2"], near_margin=margin,
+                              idx_bytes=idx_bytes)
     assert sub.near is not None and sub.near[2].numel() < sub.n_items
     st_, ct, it = cells_members(sph, L3, nseg)
     g = oz.Geometry(sph.astype(np.float32), int(c["nstructures"]), L3, nseg, st_, ct, it, c["D"], c["T2"],
@@ -463,3 +471,37 @@ def test_batch_sort_equals_per_job_sorts(eng):
             lab = np.where((lab < 0) | (lab >= nl), nl - 1, lab)
             key = key + lab * nbins
         assert np.all(np.diff(key) >= 0)
+
+
+@pytest.mark.parametrize("idx_bytes", [2, 4])
+def test_index_lists_with_shuffled_sphere_order(eng, idx_bytes):
+    """Spheres given out of structure order (a seeded shuffle of the overlap
+    fixture's 24 spheres over 3 structures): the index form sorts them into
+    records by structure, and the fused walk still equals the oracle on the
+    shuffled input bit for bit (positions, Phi, labels, flags)."""
+    c = load("dwi_overlap")
+    perm = np.random.default_rng(5).permutation(c["spheres"].shape[1])
+    sph = c["spheres"][:, perm]
+    assert not np.all(np.diff(sph[4]) >= 0)
+    L3, nseg = tuple(c["L"]), tuple(int(v) for v in c["nseg"])
+    sub = eng.DeviceSubstrate(sph, int(c["nstructures"]), L3, nseg, c["D"], c["T2"], near_margin=0.4,
+                              idx_bytes=idx_bytes)
+    st_, ct, it = cells_members(sph, L3, nseg)
+    g = oz.Geometry(sph.astype(np.float32), int(c["nstructures"]), L3, nseg, st_, ct, it, c["D"], c["T2"],
+                    dL=tuple(c["dL"]))
+    N, nt, dt = int(c["N"]), int(c["nt"]), float(c["dt"])
+    x0 = c["x0"].astype(np.float32)
+    spins, spins0, phi = x0.copy(), x0.copy(), np.zeros((6, N), np.float32)
+    r = oz.walk_f32(g, oz.philox(23), oz.MODE_PHI, spins, spins0, 0, nt, dt, G=c["G"], Garea=c["Garea"], phi=phi)
+    x = _dev(x0)
+    wk = eng.Walkers(x, x.clone(), phi=torch.zeros((6, N), device="cuda"),
+                     label=torch.full((N,), -1, dtype=torch.int32, device="cuda"),
+                     flags=torch.zeros(N, dtype=torch.int32, device="cuda"))
+    st = eng.FusedState.from_walkers(wk)
+    eng.walk_fused(sub, st, eng.L.MODE_PHI, dt, _dev(c["G"].astype(np.float32)), _dev(c["Garea"].astype(np.float32)),
+                   0, nt, eng.philox_draws(23))
+    st.to_walkers(wk)
+    np.testing.assert_array_equal(wk.spins.cpu().numpy(), spins)
+    np.testing.assert_array_equal(wk.phi.cpu().numpy(), phi)
+    np.testing.assert_array_equal(wk.label.cpu().numpy(), r["label"])
+    np.testing.assert_array_equal(wk.flags.cpu().numpy(), r["flags"])
