@@ -206,6 +206,32 @@ int nz_cells_gather(const float* spheres, int S, const int* items, int n_items, 
 int nz_cells_index(const int* items, int n_items, const int* perm, int S, const int* cell_start,
                    const int* cell_count, int ncell, void* idx, int idx_bytes, void* stream);
 
+/* ---- a12: substrate ingestion on the device — split_matrix_to_list
+ * (utils/common_utils.py:41-55) and createBoundaryZ / create_pad
+ * (utils/adjust_geometry.py:3-36), as the simulation driver applies them
+ * (cli/simulation_main.py:37-54).  rows: the pickle's matrix [M][5]
+ * (x, y, z, r, fibre id), float64, row major, on the device. ----
+ *
+ * Scratch of nz_ingest_split (M rows) and nz_ingest_plan (M = F fibres). */
+size_t nz_ingest_scratch_bytes(int M);
+/* Fibre k ends at row ends[k], the k-th row whose z equals L/2 exactly;
+ * *n_fibres (one device int) = F.  ends: [M] ints. */
+int nz_ingest_split(const double* rows, int M, double L, int* ends, int* n_fibres, void* scratch,
+                    size_t scratch_bytes, void* stream);
+/* partner[k]: the last fibre whose last row's (x, y) equals fibre k's first
+ * row's (x, y), or -1; out_offset[k]: first output row of fibre k (its rows,
+ * plus `pad` rows when it has a partner); *n_out = the output row count;
+ * *n_bad = padded fibres where it or its partner has fewer than pad/2 rows
+ * (the reference's create_pad fails on them).  partner, out_offset: [F]. */
+int nz_ingest_plan(const double* rows, const int* ends, int F, int pad, int* partner, int* out_offset, int* n_out,
+                   int* n_bad, void* scratch, size_t scratch_bytes, void* stream);
+/* The padded fibres, concatenated: out_rows [S][5] as createBoundaryZ returns
+ * them (partner rows shifted by -/+Lz, fibre ids truncated to integers), and,
+ * when spheres is not NULL, the walk's [5, S] layout (x, y, z, r, fibre
+ * index as the structure id). */
+int nz_ingest_write(const double* rows, const int* ends, int F, const int* partner, const int* out_offset, int S,
+                    double Lz, int pad, double* out_rows, double* spheres, void* stream);
+
 /* ---- a7: seeding — seedSpinsKernel (sim3d_kernel.cu:240-337) + SimGeometry3D.gpu_seed
  * (geometry.py:73-174).  target[k] != 0 marks structure k (k = nstructures is the
  * box) as a target.  A position is accepted when the first structure in id order

@@ -77,6 +77,10 @@ SIGNATURES = {
     "nz_segments_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _i, _P, _P]),
     "nz_cells_gather": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _P, _P]),
     "nz_cells_index": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _i, _P]),
+    "nz_ingest_scratch_bytes": (ctypes.c_size_t, [_i]),
+    "nz_ingest_split": (_i, [_P, _i, _d, _P, _P, _P, ctypes.c_size_t, _P]),
+    "nz_ingest_plan": (_i, [_P, _P, _i, _i, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]),
+    "nz_ingest_write": (_i, [_P, _P, _i, _P, _P, _i, _d, _i, _P, _P, _P]),
     "nz_seed": (_i, [_P, _P, _i, _u, _u, _u, _i, _P, _P, _P, _P]),
     "nz_seed_range": (_i, [_P, _P, _u, _i, _u, _u, _u, _i, _P, _P, _P, _P]),
     "nz_walk_step": (_i, [_P, _P, _i, _f, _f, _f, _i, _P, _P]),

@@ -124,6 +124,59 @@ def bound_z(fibers: list, Lz: float) -> list:
     return out
 
 
+def ingest_on_device(matrix, L: float, Lz: float | None = None, pad: int = 50):
+    """split_fibers + bound_z on the GPU (nz_ingest_split / plan / write):
+    the matrix [M, 5] (x, y, z, r, fibre id; numpy or a torch tensor) is
+    split at z == L/2 and its fibres z-padded from their partners.  Returns
+    (rows [S, 5] float64 as bound_z returns them, concatenated; spheres
+    [5, S] float64 with the fibre index as structure id; fibre lengths
+    [F] int64 on the host), the arrays on the device.  Lz defaults to L."""
+    import ctypes
+    import torch
+    from . import _lib as lib_
+    from .engine import _p, _stream, require_cuda
+    require_cuda()
+    lib = lib_.load()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    A = torch.as_tensor(matrix, dtype=torch.float64).to(dev).contiguous()
+    if A.ndim != 2 or A.shape[1] != 5:
+        raise lib_.NozomiError(f"substrate matrix must be [M, 5], got {tuple(A.shape)}")
+    M = int(A.shape[0])
+    Lz = float(L) if Lz is None else float(Lz)
+    scratch = torch.empty(max(1, int(lib.nz_ingest_scratch_bytes(M))), dtype=torch.uint8, device=dev)
+    ends = torch.empty(max(M, 1), dtype=torch.int32, device=dev)
+    counts = torch.zeros(3, dtype=torch.int32, device=dev)  # fibres, output rows, short padded fibres
+    c = ctypes.c_void_p
+    lib_.check(lib.nz_ingest_split(_p(A), M, float(L), _p(ends), c(counts.data_ptr()), _p(scratch), scratch.numel(),
+                                   _stream()), "nz_ingest_split")
+    F = int(counts[0].item())
+    partner = torch.empty(max(F, 1), dtype=torch.int32, device=dev)
+    offset = torch.empty(max(F, 1), dtype=torch.int32, device=dev)
+    lib_.check(lib.nz_ingest_plan(_p(A), _p(ends), F, int(pad), _p(partner), _p(offset), c(counts.data_ptr() + 4),
+                                  c(counts.data_ptr() + 8), _p(scratch), scratch.numel(), _stream()), "nz_ingest_plan")
+    h = counts.cpu().numpy()
+    if h[2]:
+        raise lib_.NozomiError(f"{int(h[2])} fibre(s) continue through the z face with fewer than {pad // 2} "
+                               "spheres in them or in their partner")
+    S = int(h[1])
+    rows = torch.empty((S, 5), dtype=torch.float64, device=dev)
+    spheres = torch.empty((5, S), dtype=torch.float64, device=dev)
+    lib_.check(lib.nz_ingest_write(_p(A), _p(ends), F, _p(partner), _p(offset), S, Lz, int(pad), _p(rows),
+                                   _p(spheres), _stream()), "nz_ingest_write")
+    off = offset[:F].cpu().numpy().astype(np.int64)
+    lengths = np.diff(np.append(off, S))
+    return rows, spheres, lengths
+
+
+def from_pickle_device(path) -> Substrate:
+    """from_pickle with the split and the z padding done on the GPU."""
+    arr, L, box = load_pickle(path)
+    rows, _, lengths = ingest_on_device(arr, L, box[2])
+    r = rows.cpu().numpy()
+    fibers = [f[:, :4] for f in np.split(r, np.cumsum(lengths)[:-1])] if len(lengths) else []
+    return Substrate(fibers, box, {"source": str(path), "ingested": "device"})
+
+
 def from_pickle(path) -> Substrate:
     """The simulation driver's ingestion (simulation_main.py:37-54)."""
     arr, L, box = load_pickle(path)

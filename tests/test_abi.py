@@ -212,6 +212,18 @@ def test_invalid_arguments_rejected_without_gpu():
     occ = ctypes.c_int(0)
     refused(lib.nz_batch_occupancy(_lib.MODE_PHI | _lib.LIST_IDX16 | _lib.LIST_IDX32, 128, ctypes.byref(occ)),
             "nz_batch_occupancy")
+    # ingestion: scratch sizes, small scratch, odd pads, missing arrays
+    pad = lambda b: (b + 255) // 256 * 256  # noqa: E731
+    assert lib.nz_ingest_scratch_bytes(100_000) == 2 * pad(400_000) + 2 * pad(4 * 13)
+    need = lib.nz_ingest_scratch_bytes(1000)
+    refused(lib.nz_ingest_split(FAKE, 1000, 10.0, FAKE, FAKE, FAKE, need - 1, None), "nz_ingest_split",
+            _lib.NZ_ERR_CAPACITY)
+    refused(lib.nz_ingest_split(None, 1000, 10.0, FAKE, FAKE, FAKE, need, None), "nz_ingest_split")
+    refused(lib.nz_ingest_plan(FAKE, FAKE, 10, 49, FAKE, FAKE, FAKE, FAKE, FAKE, need, None), "nz_ingest_plan")
+    refused(lib.nz_ingest_plan(FAKE, FAKE, 1000, 50, FAKE, FAKE, FAKE, FAKE, FAKE, 16, None), "nz_ingest_plan",
+            _lib.NZ_ERR_CAPACITY)
+    refused(lib.nz_ingest_write(FAKE, FAKE, 0, FAKE, FAKE, 10, 10.0, 50, FAKE, None, None), "nz_ingest_write")
+    assert lib.nz_ingest_write(None, None, 0, None, None, 0, 10.0, 50, None, None, None) == 0
     # moments walk: scratch below [steps][3][N] floats, or an unsupported mode
     small = lib.nz_walk_fused_moments_scratch_bytes(N, 100) - 4
     refused(lib.nz_walk_fused_moments(by(sub), by(a), 0, 0.01, None, None, 0, 100, by(draws), FAKE, small, FAKE,
