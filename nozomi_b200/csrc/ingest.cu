@@ -182,15 +182,15 @@ extern "C" int nz_ingest_plan(const double* rows, const int* ends, int F, int pa
                               int* n_out, int* n_bad, void* scratch, size_t scratch_bytes, void* stream) {
   if (F < 0 || pad < 0 || pad % 2 || !n_out || !n_bad || (F > 0 && (!rows || !ends || !partner || !out_offset)))
     return set_error(NZ_ERR_ARG, "nz_ingest_plan: bad arguments (F=%d pad=%d)", F, pad);
+  const size_t need = nz_ingest_scratch_bytes(F);
+  if (F > 0 && (!scratch || scratch_bytes < need))
+    return set_error(NZ_ERR_CAPACITY, "nz_ingest_plan: scratch %zu bytes < %zu", scratch_bytes, need);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(n_bad, 0, sizeof(int), st) != cudaSuccess) return check_launch("nz_ingest_plan memset");
   if (F == 0) {
     if (cudaMemsetAsync(n_out, 0, sizeof(int), st) != cudaSuccess) return check_launch("nz_ingest_plan memset");
     return NZ_OK;
   }
-  const size_t need = nz_ingest_scratch_bytes(F);
-  if (!scratch || scratch_bytes < need)
-    return set_error(NZ_ERR_CAPACITY, "nz_ingest_plan: scratch %zu bytes < %zu", scratch_bytes, need);
   char* p = static_cast<char*>(scratch);
   const size_t nf = align256i(size_t(F) * sizeof(int));
   int* len = reinterpret_cast<int*>(p);
