@@ -13,7 +13,7 @@
 // fibre id column of the result is its own ids (last pad/2, all, first
 // pad/2), every fibre's ids truncated to integers.
 //
-// Three launches stages, two host reads of a size in between:
+// Three stages, with two host reads of a size in between:
 //   nz_ingest_split  split rows and fibre count
 //   nz_ingest_plan   partner of every fibre and output offsets
 //   nz_ingest_write  the padded fibres (rows, as the reference returns them)
