@@ -49,6 +49,7 @@ extern "C" {
 #define NZ_FLAG_DRAWS_EXHAUSTED 1
 #define NZ_FLAG_ITER_CAP 2
 #define NZ_FLAG_UNSEEDED 4
+#define NZ_FLAG_BOUNDS 8    /* bounds-checked build only: an index was out of range (the access was skipped) */
 
 /* Box [-L/2, L/2]^3 and uniform cell grid: the reference kernel's template
  * constants Lx..Lz, dLx..dLz, nLx..nLz (sim3d_kernel.cu:17-28). */
@@ -104,6 +105,10 @@ typedef struct nz_substrate {
     const float* rec4;         /* [S][4], 16-byte aligned */
     const int* rec_sid;        /* [S] */
     const int* sid_start;      /* [nstructures + 2] */
+    /* Entries of the cell lists and of the near lists (0: not given).  Only
+     * the bounds-checked build reads them, to check every list range. */
+    int n_items;
+    int near_items;
 } nz_substrate;
 
 /* Source of the normal draws: an injected table normals[N][nsteps][maxk]

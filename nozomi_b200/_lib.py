@@ -8,12 +8,19 @@ from __future__ import annotations
 import ctypes
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libnozomi_b200.so"
+import os
+
+# NOZOMI_B200_DEBUG_BOUNDS=1 loads the bounds-checked build instead: every
+# cell index, list range and sphere index is checked before use, and a miss
+# sets FLAG_BOUNDS on the walker (its access skipped) rather than reading
+# out of range.  For tests and debugging; it is slower.
+DEBUG_BOUNDS = os.environ.get("NOZOMI_B200_DEBUG_BOUNDS", "") not in ("", "0")
+LIB_PATH = Path(__file__).resolve().parent / ("libnozomi_b200_debug.so" if DEBUG_BOUNDS else "libnozomi_b200.so")
 
 NZ_OK, NZ_ERR_ARG, NZ_ERR_CUDA, NZ_ERR_CAPACITY, NZ_ERR_UNSEEDED = 0, 1, 2, 3, 4
 MODE_SIG, MODE_PHASE, MODE_PHI, MODE_MOMENTS, MODE_TANGENT64 = 1, 2, 4, 8, 16
 LIST_IDX16, LIST_IDX32 = 64, 128  # nz_walk_batch: the jobs' list format (none: per-entry records)
-FLAG_DRAWS_EXHAUSTED, FLAG_ITER_CAP, FLAG_UNSEEDED = 1, 2, 4
+FLAG_DRAWS_EXHAUSTED, FLAG_ITER_CAP, FLAG_UNSEEDED, FLAG_BOUNDS = 1, 2, 4, 8
 FUSED_THREADS = 128       # walkers per CTA / per work item of the fused and batched walks
 MOMENT_STEPS = 256        # steps per launch when the fused walk accumulates moments
 SCAN_SINGLE_KEYS = 32768  # nz_state_sort scans up to this many bins in one kernel, beyond it in three
@@ -35,7 +42,7 @@ class Substrate(ctypes.Structure):
                 ("cell_count", _P), ("cell_items", _P), ("cell_sph4", _P), ("cell_sid", _P), ("D", _P),
                 ("T2", _P), ("near_margin", _f), ("near_start", _P), ("near_count", _P), ("near_sph4", _P),
                 ("near_sid", _P), ("idx_bytes", _i), ("cell_idx", _P), ("near_idx", _P), ("rec4", _P),
-                ("rec_sid", _P), ("sid_start", _P)]
+                ("rec_sid", _P), ("sid_start", _P), ("n_items", _i), ("near_items", _i)]
 
 
 class Draws(ctypes.Structure):
@@ -119,7 +126,8 @@ def load(require_built: bool = True) -> ctypes.CDLL:
     global _lib
     if _lib is None:
         if not LIB_PATH.exists():
-            raise NozomiError(f"{LIB_PATH} is missing: build it with `python -m nozomi_b200.build`")
+            raise NozomiError(f"{LIB_PATH} is missing: build it with `python -m nozomi_b200.build`"
+                              + (" --debug" if DEBUG_BOUNDS else ""))
         lib = ctypes.CDLL(str(LIB_PATH))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(lib, name)

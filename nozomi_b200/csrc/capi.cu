@@ -84,6 +84,8 @@ extern "C" int nz_walk_step(const nz_substrate* sub, const nz_walkers* wk, int m
   a.nstructures = sub->nstructures;
   a.S = sub->S;
   a.N = wk->N;
+  a.ncell = sub->grid.nx * sub->grid.ny * sub->grid.nz;
+  a.n_items = sub->n_items;
   a.spheres = sub->spheres;
   a.cell_start = sub->cell_start;
   a.cell_count = sub->cell_count;

@@ -22,6 +22,7 @@ int check_grid(const nz_grid* g, const char* who);
 struct PlainArgs {
   Grid g;
   int nstructures, S, N;
+  int ncell, n_items;  // checked by the bounds-checked build (n_items 0: unknown)
   const float* spheres;  // [5, S]: cx, cy, cz, r, structure id
   const int* cell_start;
   const int* cell_count;
@@ -95,6 +96,8 @@ struct JobDev {
   const int* rec_sid;
   const int* sid_start;
   int S;
+  // checked by the bounds-checked build (list lengths 0: unknown)
+  int ncell, n_items, near_items;
 };
 
 __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, const float* Garea, int nsteps, float dt,

@@ -20,7 +20,17 @@ enum : int {
   kFlagDrawsExhausted = 1,  // injected normal table ran out; the draw read 0
   kFlagIterCap = 2,         // a step ended at the 100-iteration cap
   kFlagUnseeded = 4,        // seeding gave up after its round limit
+  kFlagBounds = 8,          // bounds-checked build: an index was out of range and its access skipped
 };
+
+// The bounds-checked build (-DNZ_DEBUG_BOUNDS=1, libnozomi_b200_debug.so):
+// cell indices, list ranges and sphere / record indices are checked before
+// they are used; an index out of range sets kFlagBounds and its access is
+// skipped.  Nothing traps.  The default build checks nothing.
+#ifndef NZ_DEBUG_BOUNDS
+#define NZ_DEBUG_BOUNDS 0
+#endif
+constexpr bool kCheckBounds = NZ_DEBUG_BOUNDS != 0;
 
 // MIN / MAX exactly as the reference macros (sim3d_kernel.cu:7-8), NaN
 // behaviour included.

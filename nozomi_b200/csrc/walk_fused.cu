@@ -49,16 +49,26 @@ struct ScanOut {
 // One list entry: its sphere's record and a key.  Record lists (LK 0): the
 // record inline, the key the structure id (-1 for a walker in the box, which
 // reads none).  Index lists (LK 2 or 4): the key the record index, the record
-// read from the substrate's record array.
+// read from the substrate's record array.  In the bounds-checked build a
+// record index outside [0, S) sets oob and reads nothing: the entry becomes
+// a NaN record that is neither near nor containing, with a key that stops
+// nothing.
 template <int LK>
 __device__ __forceinline__ void entry(const void* __restrict__ list, const float4* __restrict__ rec,
-                                      const int* __restrict__ sid, int k, bool box, int& key, float4& c) {
+                                      const int* __restrict__ sid, int k, bool box, int S, int& oob, int& key,
+                                      float4& c) {
   if constexpr (LK == 0) {
     key = box ? -1 : __ldg(sid + k);
     c = __ldg(rec + k);
   } else {
     if constexpr (LK == 2) key = int(__ldg(static_cast<const unsigned short*>(list) + k));
     else key = __ldg(static_cast<const int*>(list) + k);
+    if (kCheckBounds && (key < 0 || key >= S)) {
+      oob = 1;
+      key = -1;
+      c = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+      return;
+    }
     c = __ldg(rec + key);
   }
 }
@@ -74,7 +84,7 @@ template <int LK, bool T64>
 __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const float4* __restrict__ rec,
                                           const int* __restrict__ sid, int start, int count, int nstructures,
                                           int lo, int hi, float x, float y, float z, int L, float a, float jx,
-                                          float jy, float jz, float reach, ScanOut& o) {
+                                          float jy, float jz, float reach, int S, int& oob, ScanOut& o) {
   o.fin = 0.0f;
   o.fout = kBig;
   o.any_in = false;
@@ -93,7 +103,7 @@ __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const f
     for (int i = 0; i < m && !stop; ++i) {
       int key;
       float4 c;
-      entry<LK>(list, rec, sid, start + base + i, box, key, c);
+      entry<LK>(list, rec, sid, start + base + i, box, S, oob, key, c);
       const bool valid = LK == 0 ? key <= L : (box || key < hi);
       stop |= !valid;
       const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
@@ -110,7 +120,7 @@ __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const f
       near_mask &= near_mask - 1;
       int key;
       float4 c;
-      entry<LK>(list, rec, sid, start + base + i, box, key, c);
+      entry<LK>(list, rec, sid, start + base + i, box, S, oob, key, c);
       const bool below = LK == 0 ? key < L : (box || key < lo);
       const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
       const float d2 = dx * dx + dy * dy + dz * dz;
@@ -137,7 +147,7 @@ __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const f
 template <int LK>
 __device__ __forceinline__ int label_of(const void* __restrict__ list, const float4* __restrict__ rec,
                                         const int* __restrict__ sid, const int* __restrict__ rec_sid, int start,
-                                        int count, int nstructures, float x, float y, float z) {
+                                        int count, int nstructures, float x, float y, float z, int S, int& oob) {
   int L = nstructures;
   for (int i = 0; i < count; ++i) {
     if constexpr (LK == 0) {
@@ -149,7 +159,7 @@ __device__ __forceinline__ int label_of(const void* __restrict__ list, const flo
     } else {
       int key;
       float4 c;
-      entry<LK>(list, rec, sid, start + i, false, key, c);
+      entry<LK>(list, rec, sid, start + i, false, S, oob, key, c);
       if (inside_test(x - c.x, y - c.y, z - c.z, c.w) < 0) return __ldg(rec_sid + key);
     }
   }
@@ -175,6 +185,26 @@ __device__ __forceinline__ int step_cell(const Grid& g, float x, float y, float 
   loy = cy * g.dLy - g.Ly / 2;
   loz = cz * g.dLz - g.Lz / 2;
   return c;
+}
+
+// Start and count of cell `cell`'s list (the near list when near).  In the
+// bounds-checked build a cell outside the grid, or a range outside the list,
+// gives an empty list and sets oob.
+__device__ __forceinline__ void cell_list(const JobDev& J, bool near, int cell, int& start, int& count, int& oob) {
+  if (kCheckBounds && (cell < 0 || cell >= J.ncell)) {
+    oob = 1;
+    start = count = 0;
+    return;
+  }
+  start = __ldg((near ? J.near_start : J.cell_start) + cell);
+  count = __ldg((near ? J.near_count : J.cell_count) + cell);
+  if (kCheckBounds) {
+    const int n = near ? J.near_items : J.n_items;
+    if (start < 0 || count < 0 || (n > 0 && start + count > n)) {
+      oob = 1;
+      start = count = 0;
+    }
+  }
 }
 
 // Draw `draw` of step s scaled by ds.
@@ -232,10 +262,10 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
   // start of a step differs from the one it was computed for
   int ds_label = label;
   float ds = sqrtf(2 * __ldg(J.D + label) * dt);
+  int oob = 0;  // bounds-checked build: an index was out of range
   if (s < s1) {
     cell = step_cell(J.g, x, y, z, lox, loy, loz);
-    pstart = __ldg((has_near ? J.near_start : J.cell_start) + cell);
-    pcount = __ldg((has_near ? J.near_count : J.cell_count) + cell);
+    cell_list(J, has_near, cell, pstart, pcount, oob);
     jump_of(J, wid, s, 0, ds, jx, jy, jz);
     draw = 1;
   }
@@ -259,15 +289,16 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     const float4* sph4 = LK ? J.rec4 : (near ? J.near_sph4 : J.sph4);
     const int* sidv = LK ? nullptr : (near ? J.near_sid : J.sid);
     int start = pstart, count = pcount;
-    if (has_near && !near) {
-      start = __ldg(J.cell_start + cell);
-      count = __ldg(J.cell_count + cell);
-    }
+    if (has_near && !near) cell_list(J, false, cell, start, count, oob);
     ScanOut r;
     constexpr bool kT64 = (MODE & NZ_MODE_TANGENT64) != 0;
     if (!scan_cell<LK, kT64>(list, sph4, sidv, start, count, J.nstructures, lo, hi, x, y, z, label, a, jx, jy, jz,
-                             reach, r)) {
-      label = label_of<LK>(list, sph4, sidv, J.rec_sid, start, count, J.nstructures, x, y, z);
+                             reach, J.S, oob, r)) {
+      label = label_of<LK>(list, sph4, sidv, J.rec_sid, start, count, J.nstructures, x, y, z, J.S, oob);
+      if (kCheckBounds && (label < 0 || label > J.nstructures)) {
+        oob = 1;
+        label = J.nstructures;
+      }
       if (LK) label_bounds(J, label, lo, hi);
       if (niter == 1) {  // the first draw's length depends on the label
         ds = sqrtf(2 * __ldg(J.D + label) * dt);
@@ -277,9 +308,10 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
         reach = sqrtf(a) * jr;
       }
       // the full list: the near one was chosen for the old reach
-      const int fs = __ldg(J.cell_start + cell), fc = __ldg(J.cell_count + cell);
+      int fs, fc;
+      cell_list(J, false, cell, fs, fc, oob);
       scan_cell<LK, kT64>(LK ? J.idx : nullptr, LK ? J.rec4 : J.sph4, LK ? nullptr : J.sid, fs, fc, J.nstructures, lo,
-                          hi, x, y, z, label, a, jx, jy, jz, reach, r);
+                          hi, x, y, z, label, a, jx, jy, jz, reach, J.S, oob, r);
     }
     jc = ref_min(jc, r.any_in ? r.fin : kBig);
     jc = ref_min(jc, r.fout);
@@ -369,8 +401,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
         ds_label = label;
       }
       cell = step_cell(J.g, x, y, z, lox, loy, loz);
-      pstart = __ldg((has_near ? J.near_start : J.cell_start) + cell);
-      pcount = __ldg((has_near ? J.near_count : J.cell_count) + cell);
+      cell_list(J, has_near, cell, pstart, pcount, oob);
     }
     if (s < s1) jump_of(J, wid, next_step, next_draw, ds, jx, jy, jz);
   }
@@ -380,6 +411,10 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
   if (MODE & NZ_MODE_PHI) {
     float4* c = J.comp + w;
     *c = make_float4(kx, ky, kz, c->w);
+  }
+  if (kCheckBounds && oob) {
+    float4* c = J.comp + w;
+    c->w = __int_as_float(__float_as_int(c->w) | kFlagBounds);
   }
 }
 
@@ -517,6 +552,9 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
   j.rec_sid = sub.rec_sid;
   j.sid_start = sub.sid_start;
   j.S = sub.S;
+  j.ncell = sub.grid.nx * sub.grid.ny * sub.grid.nz;
+  j.n_items = sub.n_items;
+  j.near_items = sub.near_items;
   j.D = sub.D;
   j.T2 = sub.T2;
   j.G = G;

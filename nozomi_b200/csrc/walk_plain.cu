@@ -34,8 +34,17 @@ __global__ void __launch_bounds__(256) walk_plain_kernel(const PlainArgs a) {
   float jump_current, jump_remaining = 1.0f;
 
   const int idxSeg = cell_of(a.g, x, y, z);
-  const int start = __ldg(a.cell_start + idxSeg);
-  const int count = __ldg(a.cell_count + idxSeg);
+  int start = 0, count = 0;
+  if (!kCheckBounds || (idxSeg >= 0 && idxSeg < a.ncell)) {
+    start = __ldg(a.cell_start + idxSeg);
+    count = __ldg(a.cell_count + idxSeg);
+  } else {
+    flags |= kFlagBounds;
+  }
+  if (kCheckBounds && (start < 0 || count < 0 || (a.n_items > 0 && start + count > a.n_items))) {
+    flags |= kFlagBounds;
+    start = count = 0;
+  }
   const int* __restrict__ items = a.cell_items + start;
 
   int niter = 0, nscatter = 0, draw = 0;
@@ -48,11 +57,19 @@ __global__ void __launch_bounds__(256) walk_plain_kernel(const PlainArgs a) {
     spinSID = a.nstructures;
     for (int n = 0; n < count; n++) {
       const int s = __ldg(items + n);
+      if (kCheckBounds && (s < 0 || s >= S)) {
+        flags |= kFlagBounds;
+        continue;
+      }
       const float sid = __ldg(sphSID + s);
       if (sid < spinSID) {
         const float isIn = inside_test(x - __ldg(cx + s), y - __ldg(cy + s), z - __ldg(cz + s), __ldg(rr + s));
         if (isIn < 0) spinSID = int(sid);
       }
+    }
+    if (kCheckBounds && (spinSID < 0 || spinSID > a.nstructures)) {
+      flags |= kFlagBounds;
+      spinSID = a.nstructures;
     }
 
     if (niter == 1) {
@@ -70,6 +87,7 @@ __global__ void __launch_bounds__(256) walk_plain_kernel(const PlainArgs a) {
     float closest_fstep_out = kBig;
     for (int n = 0; n < count; n++) {
       const int s = __ldg(items + n);
+      if (kCheckBounds && (s < 0 || s >= S)) continue;  // flagged in the label pass
       const float sid = __ldg(sphSID + s);
       if (sid > spinSID) continue;
       const float dx = x - __ldg(cx + s), dy = y - __ldg(cy + s), dz = z - __ldg(cz + s);

@@ -183,6 +183,7 @@ class DeviceSubstrate:
             raise NozomiError(f"near margin {margin} must lie in (0, {self.jump_tol})")
         st, ct, it, n = self._build_cells(margin, store=False)
         dev = _dev()
+        self.near_n = n
         if self.idx_bytes:
             self.near_margin = margin
             self.near = (st, ct, it, None, None, self._index(st, ct, it, n))
@@ -243,11 +244,13 @@ class DeviceSubstrate:
         s = L.Substrate(self.grid, self.nstructures, self.S, self.spheres.data_ptr(), self.cell_start.data_ptr(),
                         self.cell_count.data_ptr(), self.cell_items.data_ptr(), ptr(self.cell_sph4),
                         ptr(self.cell_sid), self.D.data_ptr(), self.T2.data_ptr())
+        s.n_items = int(self.n_items)
         if self.near is not None:
             st, ct, _, sph4, sid, nidx = self.near
             s.near_margin = self.near_margin
             s.near_start, s.near_count = st.data_ptr(), ct.data_ptr()
             s.near_sph4, s.near_sid, s.near_idx = ptr(sph4), ptr(sid), ptr(nidx)
+            s.near_items = int(self.near_n)
         if self.idx_bytes:
             s.idx_bytes, s.cell_idx = self.idx_bytes, self.cell_idx.data_ptr()
             s.rec4, s.rec_sid, s.sid_start = self.rec4.data_ptr(), self.rec_sid.data_ptr(), self.sid_start.data_ptr()
