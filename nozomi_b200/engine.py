@@ -135,8 +135,10 @@ class DeviceSubstrate:
         perm = np.empty(self.S, np.int32)
         perm[order] = np.arange(self.S, dtype=np.int32)
         rec_sid = sid[order].astype(np.int32)
-        self.rec4 = torch.from_numpy(np.ascontiguousarray(sph64[:4, order].T.astype(np.float32))).to(dev)
-        self.rec_sid = torch.from_numpy(rec_sid).to(dev)
+        rec4 = np.zeros((max(self.S, 1), 4), np.float32)  # one row at least: a device pointer even for S = 0
+        rec4[:self.S] = sph64[:4, order].T
+        self.rec4 = torch.from_numpy(rec4).to(dev)
+        self.rec_sid = torch.from_numpy(np.concatenate([rec_sid, np.zeros(self.S == 0, np.int32)])).to(dev)
         self.sid_start = torch.from_numpy(
             np.searchsorted(rec_sid, np.arange(self.nstructures + 2)).astype(np.int32)).to(dev)
         self.perm = torch.from_numpy(perm).to(dev)
