@@ -76,6 +76,26 @@ def box_grid(L3, nseg) -> L.Grid:
                   np.float32(Lz / nz), nx, ny, nz)
 
 
+def record_order(sph64: np.ndarray, nstructures: int):
+    """The index form's records of spheres [5, S]: the spheres sorted by
+    structure id (stable); returns rec4 [max(S, 1), 4] float32 (x, y, z, r),
+    rec_sid [max(S, 1)] int32, sid_start [nstructures + 2] int32 (the first
+    record of each structure, S at the end) and perm [max(S, 1)] int32 (each
+    sphere's record).  Arrays keep one row at least, so that an empty
+    substrate still has device pointers."""
+    S = sph64.shape[1]
+    sid = sph64[4].astype(np.int64)
+    order = np.argsort(sid, kind="stable")
+    perm = np.zeros(max(S, 1), np.int32)
+    perm[order] = np.arange(S, dtype=np.int32)
+    rec_sid = np.zeros(max(S, 1), np.int32)
+    rec_sid[:S] = sid[order]
+    rec4 = np.zeros((max(S, 1), 4), np.float32)
+    rec4[:S] = sph64[:4, order].T
+    sid_start = np.searchsorted(rec_sid[:S], np.arange(nstructures + 2)).astype(np.int32)
+    return rec4, rec_sid, sid_start, perm
+
+
 class DeviceSubstrate:
     """Spheres [5,S] (cx, cy, cz, r, structure id), box, cell grid, compact cell
     lists built on the GPU (DiffSim3d.set_segments, diffsim3d.py:107-174), the
@@ -126,21 +146,12 @@ class DeviceSubstrate:
             self.set_near_margin(near_margin)
 
     def _records(self, sph64: np.ndarray):
-        """The index form's record array: spheres sorted by structure id
-        (stable), their records and ids, the first record of every structure,
-        and each sphere's record index (perm)."""
+        """The index form's record array on the device (record_order)."""
         dev = _dev()
-        sid = sph64[4].astype(np.int64)
-        order = np.argsort(sid, kind="stable")
-        perm = np.empty(self.S, np.int32)
-        perm[order] = np.arange(self.S, dtype=np.int32)
-        rec_sid = sid[order].astype(np.int32)
-        rec4 = np.zeros((max(self.S, 1), 4), np.float32)  # one row at least: a device pointer even for S = 0
-        rec4[:self.S] = sph64[:4, order].T
+        rec4, rec_sid, sid_start, perm = record_order(sph64, self.nstructures)
         self.rec4 = torch.from_numpy(rec4).to(dev)
-        self.rec_sid = torch.from_numpy(np.concatenate([rec_sid, np.zeros(self.S == 0, np.int32)])).to(dev)
-        self.sid_start = torch.from_numpy(
-            np.searchsorted(rec_sid, np.arange(self.nstructures + 2)).astype(np.int32)).to(dev)
+        self.rec_sid = torch.from_numpy(rec_sid).to(dev)
+        self.sid_start = torch.from_numpy(sid_start).to(dev)
         self.perm = torch.from_numpy(perm).to(dev)
 
     def _index(self, start, count, items, n):

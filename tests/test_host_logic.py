@@ -202,3 +202,22 @@ def test_cached_substrate_built_by_several_processes_at_once(tmp_path):
     arrs = [np.load(tmp_path / f"s{i}.npy") for i in range(3)]
     assert all(np.array_equal(a, arrs[0]) for a in arrs[1:])
     assert len(list(cache.glob("bundle_*.pkl"))) == 1 and not list(cache.glob("*.tmp"))
+
+
+def test_record_order_of_the_index_lists():
+    """The index form's records: spheres sorted by structure (stable), the
+    first record of each structure, each sphere's record; an empty substrate
+    still gets one-row arrays."""
+    import numpy as np
+    from nozomi_b200.engine import record_order
+    sid = np.array([2, 0, 1, 0, 2, 1, 0], np.float64)
+    sph = np.vstack([np.arange(7) * 1.0, np.arange(7) * 2.0, np.arange(7) * 3.0, np.full(7, 0.5), sid])
+    rec4, rec_sid, sid_start, perm = record_order(sph, 3)
+    np.testing.assert_array_equal(rec_sid, [0, 0, 0, 1, 1, 2, 2])
+    np.testing.assert_array_equal(sid_start, [0, 3, 5, 7, 7])
+    np.testing.assert_array_equal(rec4[:, 0], [1, 3, 6, 2, 5, 0, 4])
+    for s in range(7):
+        np.testing.assert_array_equal(rec4[perm[s]], sph[:4, s].astype(np.float32))
+    rec4, rec_sid, sid_start, perm = record_order(np.zeros((5, 0)), 0)
+    assert rec4.shape == (1, 4) and rec_sid.shape == (1,) and perm.shape == (1,)
+    np.testing.assert_array_equal(sid_start, [0, 0])
