@@ -79,8 +79,11 @@ KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.
 PROFILED = {
     "packed": {"kernel_sha": None, "warp_inst_per_walker_step": None, "dram_bytes_per_walker_step": None,
                "capture": None},
-    "batched": {"kernel_sha": None, "warp_inst_per_walker_step": None, "dram_bytes_per_walker_step": None,
-                "capture": None},
+    "batched": {"kernel_sha": "8dac89916756376a", "warp_inst_per_walker_step": 46.448,
+                "dram_bytes_per_walker_step": 0.6636,
+                "capture": "walk_fused_kernel<PHI, idx16> launch 2 of `python bench.py --walker-scale 0.1 --steps 1 "
+                           "--warmup 1 --no-serving --no-plain --no-cpu-baseline --e2e-steps 0` (64 jobs, "
+                           "787,000,000 walker-steps): 36,554,718,980 warp instructions, 522.3 MB DRAM"},
 }
 
 
@@ -616,7 +619,7 @@ def run_packed(args):
     t_local = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
-    e2e_value = ws_per_step * args.e2e_steps / (float(t_local[0]) * 1e-3)
+    e2e_value = ws_per_step * args.e2e_steps / (float(t_local[0]) * 1e-3) if args.e2e_steps else None
     del graph
 
     line = None
@@ -656,9 +659,10 @@ def run_packed(args):
                            "cell_list_entries": dsub.n_items, "l2": "256 MiB flush between timed steps",
                            "parallelism": f"walkers sharded over {world} GPU(s) by walker-id range; "
                                           "one all-reduce of the signal sums per step"},
-                "e2e": {"value": e2e_value, "unit": "walker-steps/s",
-                        "h2d_bytes_per_step": int(x_host.numel() * x_host.element_size()),
-                        "d2h_bytes_per_step": int(out_bytes)},
+                "e2e": None if e2e_value is None else {
+                    "value": e2e_value, "unit": "walker-steps/s",
+                    "h2d_bytes_per_step": int(x_host.numel() * x_host.element_size()),
+                    "d2h_bytes_per_step": int(out_bytes)},
                 "gpu_launches": launches_per_step * args.steps,
                 "kernel": {"name": "walk_fused_kernel", "launches": n_walk, "avg_launch_ms": walk_launch_ms,
                            "walker_steps_per_launch": per_launch_ws, "kernel_walker_steps_per_s": kernel_ws_s,
