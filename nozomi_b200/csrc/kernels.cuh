@@ -54,6 +54,13 @@ constexpr int kFusedMaxThreads = 256;  // largest CTA of nz_walk_batch
 #define NZ_FUSED_MIN_BLOCKS 3
 #endif
 constexpr int kFusedMinBlocks = NZ_FUSED_MIN_BLOCKS;  // 256-thread CTAs per SM the register budget is sized for
+#ifndef NZ_SCAN_UNROLL
+#define NZ_SCAN_UNROLL 4
+#endif
+// list entries loaded together in the scan's first pass: 4 measured fastest
+// on both the batched and the packed workloads (1, 2, 4, 8 tried)
+constexpr int kScanUnroll = NZ_SCAN_UNROLL;
+static_assert(32 % kScanUnroll == 0, "the scan unroll must divide 32");
 constexpr int kMomentSteps = 256;  // steps per launch in NZ_MODE_MOMENTS (shared-memory staging)
 // Internal mode bit (nz_walk_fused_moments only): at each step end the fused
 // walk stores the walker's float displacement from its origin; a reduction

@@ -99,19 +99,34 @@ __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const f
     // at least 2.1 nm that dwarfs the rounding of d2 and r*r, so that a far
     // sphere neither contains the walker nor lies within this iteration's
     // reach; predicated, one entry per load
+    // kScanUnroll entries are loaded together, so that their loads (two
+    // dependent ones each in index form) are in flight at once; entries past
+    // the first of a higher structure are invalid too (keys ascend), so a
+    // batch never marks one near
     uint32_t near_mask = 0u;
-    for (int i = 0; i < m && !stop; ++i) {
-      int key;
-      float4 c;
-      entry<LK>(list, rec, sid, start + base + i, box, S, oob, key, c);
-      const bool valid = LK == 0 ? key <= L : (box || key < hi);
-      stop |= !valid;
-      const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
-      // a filter, not the reference's arithmetic: fused multiply-adds are
-      // fine here (their rounding is far inside the slack)
-      const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
-      const float t = c.w + slack;
-      near_mask |= (valid && d2 <= t * t) ? (1u << i) : 0u;
+    for (int i0 = 0; i0 < m && !stop; i0 += kScanUnroll) {
+      int key[kScanUnroll];
+      float4 c[kScanUnroll];
+#pragma unroll
+      for (int u = 0; u < kScanUnroll; ++u) {
+        if (kScanUnroll == 1 || i0 + u < m) {
+          entry<LK>(list, rec, sid, start + base + i0 + u, box, S, oob, key[u], c[u]);
+        } else {  // past the chunk: a NaN record, never near, stops nothing
+          key[u] = -1;
+          c[u] = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kScanUnroll; ++u) {
+        const bool valid = LK == 0 ? key[u] <= L : (box || key[u] < hi);
+        stop |= !valid;
+        const float dx = x - c[u].x, dy = y - c[u].y, dz = z - c[u].z;
+        // a filter, not the reference's arithmetic: fused multiply-adds are
+        // fine here (their rounding is far inside the slack)
+        const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+        const float t = c[u].w + slack;
+        near_mask |= (valid && d2 <= t * t) ? (1u << (i0 + u)) : 0u;
+      }
     }
     // second pass, near entries only: the reference's inside test, then the
     // fraction of a containing sphere or of a lower structure's sphere
@@ -441,8 +456,13 @@ __device__ __forceinline__ void run_item(const JobDev& J, int first, int count, 
 // value, item i = walkers [i*T, i*T + T).  Otherwise jobs and items come from
 // device arrays; with queue != null the grid is persistent and each CTA takes
 // items from *queue until none is left.
+#ifdef NZ_FUSED_MAXNREG
+#define NZ_FUSED_BOUNDS __maxnreg__(NZ_FUSED_MAXNREG)
+#else
+#define NZ_FUSED_BOUNDS __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
+#endif
 template <int MODE, int LK, bool SINGLE>
-__global__ void __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
+__global__ void NZ_FUSED_BOUNDS
     walk_fused_kernel(const __grid_constant__ JobDev single, const nz_job* __restrict__ jobs,
                       const nz_item* __restrict__ items, int n_items, int step0, int step1, int* queue) {
   __shared__ int s_item;
