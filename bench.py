@@ -77,13 +77,16 @@ KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.
 # dram__bytes_write.sum) of the captured launch, divided by the walker-steps
 # that launch ran; kernel_sha: the sources' hash at capture.
 PROFILED = {
-    "packed": {"kernel_sha": None, "warp_inst_per_walker_step": None, "dram_bytes_per_walker_step": None,
-               "capture": None},
-    "batched": {"kernel_sha": "8dac89916756376a", "warp_inst_per_walker_step": 46.448,
-                "dram_bytes_per_walker_step": 0.6636,
+    "packed": {"kernel_sha": "9ea3545037c04741", "warp_inst_per_walker_step": 64.591,
+               "dram_bytes_per_walker_step": 1.1100,
+               "capture": "walk_fused_kernel<PHI, idx16> launch 3 of `python bench.py --workload packed --walkers "
+                          "1000000 --steps-per-launch 200 --steps 1 --warmup 1 --no-cpu-baseline --e2e-steps 0` "
+                          "(200,000,000 walker-steps): 12,918,262,538 warp instructions, 222.0 MB DRAM"},
+    "batched": {"kernel_sha": "9ea3545037c04741", "warp_inst_per_walker_step": 49.074,
+                "dram_bytes_per_walker_step": 0.6649,
                 "capture": "walk_fused_kernel<PHI, idx16> launch 2 of `python bench.py --walker-scale 0.1 --steps 1 "
                            "--warmup 1 --no-serving --no-plain --no-cpu-baseline --e2e-steps 0` (64 jobs, "
-                           "787,000,000 walker-steps): 36,554,718,980 warp instructions, 522.3 MB DRAM"},
+                           "787,000,000 walker-steps): 38,621,089,270 warp instructions, 523.3 MB DRAM"},
 }
 
 
@@ -134,7 +137,8 @@ def parse(argv=None):
     ap.add_argument("--threads", type=int, default=128, help="batched: walkers per CTA")
     ap.add_argument("--plain-every", type=int, default=4, help="batched: time the plain path on every k-th job")
     ap.add_argument("--no-plain", action="store_true", help="batched: skip the plain-path comparison")
-    ap.add_argument("--autotune", action="store_true", help="batched: pick the launch shape with the autotuner")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batched: the library's default launch shape instead of the autotuner's choice")
     return ap.parse_args(argv)
 
 
@@ -783,9 +787,12 @@ def run_batched(args):
     tuning = _tuning_from_args(args, Tuning())
     tune_report = None
     threads = args.threads
-    if args.autotune:
+    if not args.no_autotune:  # the launch shape from the autotuner's short trials (cached per GPU and workload)
         from nozomi_b200.autotune import autotune
+        t0 = time.perf_counter()
         tuning, threads, tune_report = autotune(specs)
+        tune_report["seconds"] = time.perf_counter() - t0
+        tuning = _tuning_from_args(args, tuning)
     cache = SubstrateCache()
     stream = torch.cuda.current_stream()
     torch.cuda.synchronize()
@@ -956,7 +963,7 @@ def run_batched(args):
                                 "lists (wall clock); not part of value"},
             "autotune": None if tune_report is None else {
                 "cached": tune_report["cached"], "choice": {"threads": threads, **dataclasses.asdict(tuning)},
-                "trials": len(tune_report.get("trials", [])),
+                "trials": len(tune_report.get("trials", [])), "seconds": tune_report.get("seconds"),
                 "trial_walker_steps_per_s": tune_report.get("trial_walker_steps_per_s")},
             "roofline": roof_issue, "roofline_fp32": roof_fp32, "roofline_hbm": roof_hbm,
             "cpu_baseline": cpu, "clocks": clk}
