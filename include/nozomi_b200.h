@@ -237,6 +237,33 @@ int nz_ingest_plan(const double* rows, const int* ends, int F, int pad, int* par
 int nz_ingest_write(const double* rows, const int* ends, int F, const int* partner, const int* out_offset, int S,
                     double Lz, int pad, double* out_rows, double* spheres, void* stream);
 
+/* ---- substrate-generator collision detection — collide_spheres_gpu
+ * (substrate_generator/helper/CollisionDetection.py:10-62) on the grid of
+ * blocks it builds: block edges Lx/10 (grid.dLx..dLz = Lx/nx.. in float32,
+ * nx.. = ceil(L/(Lx/10)) per axis).  A sphere belongs to a block when all six
+ * boundary distances of its set_segments (:65-115) are below 1 um (float32,
+ * the reference's operation order).  A pair of spheres of different fibres
+ * collides when (r_a + r_b + buff) - |x_a - x_b| > 0 in float32; each pair is
+ * reported once, as (min, max).  Spheres that belong to no block take part
+ * in no pair.  pos: [S][3] float32; radii, fiber_id: [S] float32. ----
+ *
+ * Scratch shared by nz_collide_cells and the nz_collide_pairs that follows it. */
+size_t nz_collide_scratch_bytes(int S, const nz_grid* grid);
+/* Block ranges and member counts; *n_members (one device int) = the total
+ * number of (block, sphere) memberships, the size of nz_collide_pairs' items. */
+int nz_collide_cells(const float* pos, const float* radii, int S, const nz_grid* grid, int* n_members,
+                     void* scratch, size_t scratch_bytes, void* stream);
+/* Every colliding pair, unordered, into pairs[cap][2]; *n_pairs = how many
+ * there are (more than cap: call again with a larger buffer).  items:
+ * n_members ints of scratch for the block lists. */
+int nz_collide_pairs(const float* pos, const float* radii, const float* fiber_id, int S, const nz_grid* grid,
+                     float buff, int* items, int n_members, int* pairs, int cap, int* n_pairs, void* scratch,
+                     size_t scratch_bytes, void* stream);
+/* Pairs [n][2] with entries in [0, S) into lexicographic order (out; the
+ * order torch.unique gives the reference's rows). */
+size_t nz_pairs_sort_scratch_bytes(int S);
+int nz_pairs_sort(const int* pairs, int n, int S, int* out, void* scratch, size_t scratch_bytes, void* stream);
+
 /* ---- a7: seeding — seedSpinsKernel (sim3d_kernel.cu:240-337) + SimGeometry3D.gpu_seed
  * (geometry.py:73-174).  target[k] != 0 marks structure k (k = nstructures is the
  * box) as a target.  A position is accepted when the first structure in id order

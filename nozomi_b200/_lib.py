@@ -84,6 +84,11 @@ SIGNATURES = {
     "nz_segments_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _i, _P, _P]),
     "nz_cells_gather": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _P, _P]),
     "nz_cells_index": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _i, _P]),
+    "nz_collide_scratch_bytes": (ctypes.c_size_t, [_i, _P]),
+    "nz_collide_cells": (_i, [_P, _P, _i, _P, _P, _P, ctypes.c_size_t, _P]),
+    "nz_collide_pairs": (_i, [_P, _P, _P, _i, _P, _f, _P, _i, _P, _i, _P, _P, ctypes.c_size_t, _P]),
+    "nz_pairs_sort_scratch_bytes": (ctypes.c_size_t, [_i]),
+    "nz_pairs_sort": (_i, [_P, _i, _i, _P, _P, ctypes.c_size_t, _P]),
     "nz_ingest_scratch_bytes": (ctypes.c_size_t, [_i]),
     "nz_ingest_split": (_i, [_P, _i, _d, _P, _P, _P, ctypes.c_size_t, _P]),
     "nz_ingest_plan": (_i, [_P, _P, _i, _i, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]),

@@ -117,6 +117,11 @@ __global__ void pack_kernel(nz_walkers wk, const uint32_t* ids, nz_state st);
 __global__ void disp_moments_kernel(const float* __restrict__ disp, int N, double* __restrict__ out);
 __global__ void unpack_kernel(nz_state st, nz_walkers wk, int by_id, int* bad);
 
+// ---- ingest.cu ----
+// *total = off[F - 1] + len[F - 1] (0 when F is 0): a list's size after its scan.
+__global__ void offsets_total_kernel(const int* __restrict__ len, const int* __restrict__ off, int F,
+                                     int* __restrict__ total);
+
 // ---- cells.cu ----
 __global__ void scan_kernel(const int* __restrict__ in, int* __restrict__ out, int n, int* __restrict__ total);
 // Exclusive scan of n ints on stream st: one CTA up to kScanSingle ints,

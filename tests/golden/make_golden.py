@@ -3,10 +3,10 @@
 Run where the reference tree is present (by default a folder named
 ``reference`` beside this repository; override with NOZOMI_REFERENCE_ROOT):
 
-    python tests/golden/make_golden.py [ingestion | faces]
+    python tests/golden/make_golden.py [ingestion | faces | collision]
 
 (``ingestion`` regenerates only tests/golden/ingestion.npz, ``faces`` only
-tests/golden/dwi_faces.npz.)  The reference's own Python engine (DiffSim3d / DwiSim3d / SimGeometry3D,
+tests/golden/dwi_faces.npz, ``collision`` only tests/golden/collision.npz.)  The reference's own Python engine (DiffSim3d / DwiSim3d / SimGeometry3D,
 simulation_toolkit/simulation_engine/) is imported with a host stand-in for
 pycuda (oracle/fake_pycuda.py); its ``SourceModule`` compiles the reference's
 own template-substituted kernel source (sim3d_kernel.cu) for the CPU.  Draws are
@@ -309,7 +309,48 @@ def faces_case(ds3, geo, wf):
     dwi_case(ds3, geo, wf, "dwi_faces", tuple(L), structs, None, nseg, N, pg, dirs, 2.0, 505, custom_x0=x0)
 
 
+def collision_case():
+    """collision.npz: the reference's own collide_spheres_gpu
+    (substrate_generator/helper/CollisionDetection.py, loaded by file path,
+    run on CPU tensors) on a seeded 500-axon bundle whose sphere centres are
+    jittered (so that axons overlap), spheres inside the box only, for buff
+    0 and 0.05 um, with the closest call's distance from the threshold."""
+    import torch
+    from nozomi_b200.substrates import axon_bundle
+    from oracle.collide_oracle import margin
+    spec = importlib.util.spec_from_file_location(
+        "ref_collision", REFERENCE_ROOT / "simulation_toolkit/substrate_generator/helper/CollisionDetection.py")
+    cd = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(cd)
+    sub = axon_bundle(500, seed=11)
+    rng = np.random.default_rng(12)
+    rows = []
+    for k, f in enumerate(sub.fibers):
+        f = np.asarray(f, np.float64)
+        inside = np.all(np.abs(f[:, :3]) <= np.array(sub.L) / 2, axis=1)
+        f = f[inside]
+        rows.append(np.column_stack([f[:, :4], np.full(len(f), float(k))]))
+    A = np.concatenate(rows)
+    A[:, :2] += rng.normal(0.0, 0.3, (len(A), 2))
+    A[:, :2] = np.clip(A[:, :2], -np.array(sub.L[:2]) / 2, np.array(sub.L[:2]) / 2)
+    pos = torch.from_numpy(A[:, :3].astype(np.float32))
+    r = torch.from_numpy(A[:, 3].astype(np.float32))
+    fid = torch.from_numpy(A[:, 4].astype(np.float32))
+    Lx, Ly, Lz = (torch.tensor(float(v), dtype=torch.float32) for v in sub.L)
+    out = {"pos": pos.numpy(), "radii": r.numpy(), "fiber_id": fid.numpy(), "L": np.array(sub.L, np.float32)}
+    for i, buff in enumerate((0.0, 0.05)):
+        pairs = cd.collide_spheres_gpu(pos, r, fid, Lx, Ly, Lz, torch.tensor([buff], dtype=torch.float32))
+        out[f"buff{i}"] = np.float32(buff)
+        out[f"pairs{i}"] = pairs.numpy().astype(np.int32)
+        out[f"margin{i}"] = margin(pos.numpy(), r.numpy(), fid.numpy(), buff)
+        print("collision", buff, pairs.shape[0], "pairs, closest call", out[f"margin{i}"])
+    np.savez_compressed(OUT / "collision.npz", **out)
+
+
 def main():
+    if sys.argv[1:] == ["collision"]:
+        collision_case()
+        return
     ds3, geo, wf, ag = _load_reference()
     if sys.argv[1:] == ["ingestion"]:
         import tempfile

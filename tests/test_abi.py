@@ -212,6 +212,21 @@ def test_invalid_arguments_rejected_without_gpu():
     occ = ctypes.c_int(0)
     refused(lib.nz_batch_occupancy(_lib.MODE_PHI | _lib.LIST_IDX16 | _lib.LIST_IDX32, 128, ctypes.byref(occ)),
             "nz_batch_occupancy")
+    # collision detection: grid checks, scratch, capacities
+    cg = _lib.Grid(60.0, 60.0, 40.0, 6.0, 6.0, 5.7142857, 10, 10, 7)
+    cneed = lib.nz_collide_scratch_bytes(1000, by(cg))
+    assert cneed > 0 and lib.nz_collide_scratch_bytes(-1, by(cg)) == 0
+    refused(lib.nz_collide_cells(FAKE, FAKE, 1000, by(cg), FAKE, FAKE, cneed - 1, None), "nz_collide_cells",
+            _lib.NZ_ERR_CAPACITY)
+    refused(lib.nz_collide_cells(FAKE, FAKE, 1000, by(_lib.Grid(60.0, 60.0, 40.0, 6.0, 0.0, 5.7, 10, 10, 7)), FAKE,
+                                 FAKE, cneed, None), "nz_collide_cells")
+    refused(lib.nz_collide_pairs(FAKE, FAKE, None, 1000, by(cg), 0.0, FAKE, 50, FAKE, 10, FAKE, FAKE, cneed, None),
+            "nz_collide_pairs")
+    refused(lib.nz_collide_pairs(FAKE, FAKE, FAKE, 1000, by(cg), 0.0, FAKE, 50, None, 10, FAKE, FAKE, cneed, None),
+            "nz_collide_pairs")
+    refused(lib.nz_pairs_sort(FAKE, 10, 0, FAKE, FAKE, 1 << 20, None), "nz_pairs_sort")
+    refused(lib.nz_pairs_sort(FAKE, 10, 1000, FAKE, FAKE, 16, None), "nz_pairs_sort", _lib.NZ_ERR_CAPACITY)
+    assert lib.nz_pairs_sort(None, 0, 1000, None, None, 0, None) == 0
     # ingestion: scratch sizes, small scratch, odd pads, missing arrays
     pad = lambda b: (b + 255) // 256 * 256  # noqa: E731
     assert lib.nz_ingest_scratch_bytes(100_000) == 2 * pad(400_000) + 2 * pad(4 * 13)
