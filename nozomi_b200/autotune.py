@@ -27,10 +27,10 @@ from .waveforms import ArbitraryWaveform
 
 SPACE = {
     "threads": [64, 128, 256],
-    "cell": [0.5, 0.667, 1.0, 1.5],
+    "cell": [0.4, 0.5, 0.667, 1.0, 1.5],
     "near_margin": [0.4, 0.5, 0.6, None],
-    "steps_per_launch": [250, 500, 1000, 2000],
-    "coarsen": [2, 4, 8, 12],
+    "steps_per_launch": [500, 1000, 2000, 4000],
+    "coarsen": [4, 8, 12, 16],
 }
 CACHE_FILE = Path(os.environ.get("NOZOMI_B200_CACHE", Path.home() / ".cache" / "nozomi_b200")) / "autotune.json"
 
