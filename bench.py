@@ -121,6 +121,8 @@ def parse(argv=None):
     ap.add_argument("--coarsen", type=int, default=None)
     ap.add_argument("--by-label", type=int, default=None, help="re-bin by (label, bin): 1, or by bin only: 0")
     ap.add_argument("--near-margin", type=float, default=None, help="near-list margin in um (0: none)")
+    ap.add_argument("--near-shape", default=None, choices=["round", "box"],
+                    help="near lists by the Euclidean sphere-to-cell test (round) or the reference's box test")
     ap.add_argument("--lists", default=None, choices=["index", "records"],
                     help="the fused walk's list form: index (16/32-bit entries into one record array) or records "
                          "(per-entry sphere records)")
@@ -509,14 +511,14 @@ def run_packed(args):
     # near margin 0.5 um, re-binning bins of 8^3 cells, 2000 steps per launch
     tuning = _tuning_from_args(args, Tuning(cell=0.5, near_margin=0.5, coarsen=8, steps_per_launch=2000))
     dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin,
-                            lists=tuning.lists)
+                            lists=tuning.lists, near_shape=tuning.near_shape)
     # the one-time cell build (member lists, near lists, per-entry records) is
     # outside the metric; it is timed on a second build, the first having
     # loaded the library and warmed the allocator
     torch.cuda.synchronize()
     tb = time.perf_counter()
     dsub = device_substrate(sub, D=2.0, T2=100.0, cell=tuning.cell, near_margin=tuning.near_margin,
-                            lists=tuning.lists)
+                            lists=tuning.lists, near_shape=tuning.near_shape)
     torch.cuda.synchronize()
     cell_build_ms = (time.perf_counter() - tb) * 1e3
     amps = pg.amplitude_for_b(bvals)
@@ -658,6 +660,7 @@ def run_packed(args):
                            "cell_um": tuning.cell, "steps_per_launch": tuning.steps_per_launch,
                            "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label,
                            "near_margin_um": tuning.near_margin, "lists": tuning.lists,
+                           "near_shape": tuning.near_shape,
                            "near_list_entries": int(dsub.near[2].numel()) if dsub.near is not None else 0,
                            "spheres": sub.S, "cells": dsub.ncell,
                            "cell_list_entries": dsub.n_items, "l2": "256 MiB flush between timed steps",
@@ -700,6 +703,8 @@ def _tuning_from_args(args, base):
         base.near_margin = args.near_margin if args.near_margin > 0 else None
     if args.lists:
         base.lists = args.lists
+    if args.near_shape:
+        base.near_shape = args.near_shape
     return base
 
 
@@ -880,7 +885,8 @@ def run_batched(args):
               "walkers": sum(sp.N for sp in all_specs), "threads": threads,
               "steps_per_launch": tuning.steps_per_launch, "near_margin_um": tuning.near_margin,
               "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label,
-              "lists": tuning.lists, "persistent_grid": run.grid, "chunks": len(run.chunks),
+              "lists": tuning.lists, "near_shape": tuning.near_shape, "persistent_grid": run.grid,
+              "chunks": len(run.chunks),
               "l2": "256 MiB flush between timed steps (the inputs, 64 substrates' cell lists and walker "
                     "state, are also larger than L2)",
               "parallelism": (f"jobs sharded whole over {world} GPUs, longest first" if world > 1 else "one GPU")}

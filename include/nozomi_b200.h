@@ -191,6 +191,16 @@ int nz_exclusive_scan_i32(const int* in, int* out, int n, int* total, void* stre
 int nz_cells_fill(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz,
                   double jump_tol, const int* offsets, const int* counts, int* cursor, int* items, void* stream);
 
+/* The fused walk's near lists: nz_cells_count / nz_cells_fill with margin
+ * `margin`, keeping of each sphere's cells only those whose box lies within
+ * r + margin (+ 1e-4 um) of its centre (Euclidean), a subset of the box
+ * test that still holds every sphere a walker near the cell can touch or lie
+ * inside.  No reference counterpart (the reference has no near lists). */
+int nz_cells_count_round(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz,
+                         double margin, int* counts, void* stream);
+int nz_cells_fill_round(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny, int nz,
+                        double margin, const int* offsets, const int* counts, int* cursor, int* items, void* stream);
+
 /* The reference's padded table (diffsim3d.py:144-168): K = the largest member
  * count; cell c's K entries at segments[c*K] are the K spheres of smallest
  * in_segment (ties by lower index), ascending by index. */

@@ -81,6 +81,8 @@ SIGNATURES = {
     "nz_cells_count": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _d, _P, _P]),
     "nz_exclusive_scan_i32": (_i, [_P, _P, _i, _P, _P]),
     "nz_cells_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _d, _P, _P, _P, _P, _P]),
+    "nz_cells_count_round": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _d, _P, _P]),
+    "nz_cells_fill_round": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _d, _P, _P, _P, _P, _P]),
     "nz_segments_fill": (_i, [_P, _i, _d, _d, _d, _i, _i, _i, _i, _P, _P]),
     "nz_cells_gather": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _P, _P]),
     "nz_cells_index": (_i, [_P, _i, _P, _i, _P, _P, _i, _P, _i, _P]),

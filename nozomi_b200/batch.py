@@ -71,7 +71,7 @@ class SubstrateCache:
         self.misses = 0
 
     def get(self, key, substrate: Substrate, D, T2, tuning: Tuning) -> engine.DeviceSubstrate:
-        k = (key, float(D), float(T2), tuning.cell, tuning.near_margin, tuning.lists)
+        k = (key, float(D), float(T2), tuning.cell, tuning.near_margin, tuning.lists, tuning.near_shape)
         if k in self.items:
             self.hits += 1
             self.order.remove(k)
@@ -79,7 +79,7 @@ class SubstrateCache:
             return self.items[k]
         self.misses += 1
         d = device_substrate(substrate, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin,
-                             lists=tuning.lists)
+                             lists=tuning.lists, near_shape=tuning.near_shape)
         self.items[k] = d
         self.hosts[k] = substrate
         self.order.append(k)

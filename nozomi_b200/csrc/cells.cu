@@ -76,6 +76,60 @@ __global__ void cells_fill_kernel(const double* __restrict__ sph, int S, CellGeo
       }
 }
 
+// Rounded membership, for the fused walk's near lists: a sphere is listed in
+// a cell of its box-test window (in_segment < margin) only when the
+// Euclidean distance from its centre to the cell's box is at most
+// r + margin + 1e-4 um.  A walker in the cell (or within d of it) can touch
+// or lie inside only spheres whose centre is within r + tol + reach + d of
+// the box, and the fused walk takes the near list only while
+// (d + reach) * 1.02 + tol + 2 nm <= margin, so these lists hold every
+// sphere the walk can meet; the corners of the box test's window, about a
+// third of its entries for cells small beside the spheres, are left out.
+__device__ __forceinline__ bool within_round(double x, double y, double z, double r, const CellGeom& g, int n, int m,
+                                             int p) {
+  const double dLx = g.Lx / g.nx, dLy = g.Ly / g.ny, dLz = g.Lz / g.nz;
+  const double x0 = n * dLx - g.Lx / 2, y0 = m * dLy - g.Ly / 2, z0 = p * dLz - g.Lz / 2;
+  const double ex = fmax(fmax(x0 - x, 0.0), x - (x0 + dLx));
+  const double ey = fmax(fmax(y0 - y, 0.0), y - (y0 + dLy));
+  const double ez = fmax(fmax(z0 - z, 0.0), z - (z0 + dLz));
+  const double R = r + g.tol + 1e-4;
+  return ex * ex + ey * ey + ez * ez <= R * R;
+}
+
+__global__ void cells_count_round_kernel(const double* __restrict__ sph, int S, CellGeom g, int* __restrict__ counts) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const double x = sph[s], y = sph[S + s], z = sph[2 * S + s], r = sph[3 * S + s];
+  int x0, x1, y0, y1, z0, z1;
+  axis_range(x, r, g.Lx, g.nx, g.tol, x0, x1);
+  axis_range(y, r, g.Ly, g.ny, g.tol, y0, y1);
+  axis_range(z, r, g.Lz, g.nz, g.tol, z0, z1);
+  for (int p = z0; p <= z1; ++p)
+    for (int m = y0; m <= y1; ++m)
+      for (int n = x0; n <= x1; ++n)
+        if (within_round(x, y, z, r, g, n, m, p)) atomicAdd(counts + (size_t(p) * g.ny + m) * g.nx + n, 1);
+}
+
+__global__ void cells_fill_round_kernel(const double* __restrict__ sph, int S, CellGeom g,
+                                        const int* __restrict__ offsets, int* __restrict__ cursor,
+                                        int* __restrict__ items) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const double x = sph[s], y = sph[S + s], z = sph[2 * S + s], r = sph[3 * S + s];
+  int x0, x1, y0, y1, z0, z1;
+  axis_range(x, r, g.Lx, g.nx, g.tol, x0, x1);
+  axis_range(y, r, g.Ly, g.ny, g.tol, y0, y1);
+  axis_range(z, r, g.Lz, g.nz, g.tol, z0, z1);
+  for (int p = z0; p <= z1; ++p)
+    for (int m = y0; m <= y1; ++m)
+      for (int n = x0; n <= x1; ++n) {
+        if (!within_round(x, y, z, r, g, n, m, p)) continue;
+        const size_t c = (size_t(p) * g.ny + m) * g.nx + n;
+        const int slot = atomicAdd(cursor + c, 1);
+        items[offsets[c] + slot] = s;
+      }
+}
+
 // Heapsort of one cell's list (ascending sphere index), one thread per cell.
 __global__ void cells_sort_kernel(const int* __restrict__ offsets, const int* __restrict__ counts, int ncell,
                                   int* __restrict__ items) {
@@ -430,6 +484,39 @@ extern "C" int nz_cells_count(const double* spheres64, int S, double Lx, double 
   CellGeom g{Lx, Ly, Lz, nx, ny, nz_, jump_tol};
   cells_count_kernel<<<(S + 255) / 256, 256, 0, st>>>(spheres64, S, g, counts);
   return check_launch("cells_count_kernel");
+}
+
+extern "C" int nz_cells_count_round(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny,
+                                    int nz_, double margin, int* counts, void* stream) {
+  if (S < 0 || nx <= 0 || ny <= 0 || nz_ <= 0 || !counts || (S > 0 && !spheres64) || !(margin >= 0.0))
+    return set_error(NZ_ERR_ARG, "nz_cells_count_round: bad arguments (S=%d grid=%dx%dx%d)", S, nx, ny, nz_);
+  const size_t ncell = size_t(nx) * ny * nz_;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(counts, 0, ncell * sizeof(int), st) != cudaSuccess)
+    return check_launch("nz_cells_count_round memset");
+  if (S == 0) return NZ_OK;
+  CellGeom g{Lx, Ly, Lz, nx, ny, nz_, margin};
+  cells_count_round_kernel<<<(S + 255) / 256, 256, 0, st>>>(spheres64, S, g, counts);
+  return check_launch("cells_count_round_kernel");
+}
+
+extern "C" int nz_cells_fill_round(const double* spheres64, int S, double Lx, double Ly, double Lz, int nx, int ny,
+                                   int nz_, double margin, const int* offsets, const int* counts, int* cursor,
+                                   int* items, void* stream) {
+  if (S < 0 || nx <= 0 || ny <= 0 || nz_ <= 0 || !offsets || !counts || !cursor || (S > 0 && !spheres64) ||
+      !(margin >= 0.0))
+    return set_error(NZ_ERR_ARG, "nz_cells_fill_round: bad arguments (S=%d grid=%dx%dx%d)", S, nx, ny, nz_);
+  const size_t ncell = size_t(nx) * ny * nz_;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(cursor, 0, ncell * sizeof(int), st) != cudaSuccess)
+    return check_launch("nz_cells_fill_round memset");
+  if (S == 0) return NZ_OK;
+  CellGeom g{Lx, Ly, Lz, nx, ny, nz_, margin};
+  cells_fill_round_kernel<<<(S + 255) / 256, 256, 0, st>>>(spheres64, S, g, offsets, cursor, items);
+  int rc = check_launch("cells_fill_round_kernel");
+  if (rc != NZ_OK) return rc;
+  cells_sort_kernel<<<unsigned((ncell + 127) / 128), 128, 0, st>>>(offsets, counts, int(ncell), items);
+  return check_launch("cells_sort_kernel");
 }
 
 extern "C" int nz_exclusive_scan_i32(const int* in, int* out, int n, int* total, void* stream) {

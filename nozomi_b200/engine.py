@@ -105,10 +105,12 @@ class DeviceSubstrate:
     entry carries its sphere's centre, radius and structure id); 2 or 4, index
     lists (each entry a 16- or 32-bit index into one record array of the
     substrate, the spheres sorted by structure id); None, index lists of 16
-    bits when S <= 65536, else 32."""
+    bits when S <= 65536, else 32.  near_round: near lists by the Euclidean
+    sphere-to-cell test (the default) or the reference's box test."""
 
     def __init__(self, spheres: np.ndarray, nstructures: int, L3, nseg, D, T2, jump_tol: float = 1.0,
-                 cells: tuple | None = None, near_margin: float | None = None, idx_bytes: int | None = None):
+                 cells: tuple | None = None, near_margin: float | None = None, idx_bytes: int | None = None,
+                 near_round: bool = True):
         sph64 = np.ascontiguousarray(spheres, dtype=np.float64).reshape(5, -1)
         validate_substrate(sph64, int(nstructures), L3, nseg, D, T2)
         require_cuda()
@@ -119,6 +121,7 @@ class DeviceSubstrate:
         if idx_bytes not in (0, 2, 4) or (idx_bytes == 2 and self.S > 65536):
             raise NozomiError(f"list form idx_bytes={idx_bytes} does not suit {self.S} spheres (0, 2 up to 65536, 4)")
         self.idx_bytes = int(idx_bytes)
+        self.near_round = bool(near_round)
         self.nstructures = int(nstructures)
         self.L = tuple(float(v) for v in L3)
         self.nseg = tuple(int(v) for v in nseg)
@@ -162,15 +165,19 @@ class DeviceSubstrate:
                                         self.idx_bytes, _stream()), "nz_cells_index")
         return idx
 
-    def _build_cells(self, margin: float | None = None, store: bool = True):
+    def _build_cells(self, margin: float | None = None, store: bool = True, rounded: bool = False):
+        """Member lists with the reference's box test (margin: jump_tol by
+        default); rounded: the near lists' Euclidean test (nz_cells_*_round)."""
         dev = _dev()
         lib = L.load()
         Lx, Ly, Lz = self.L
         nx, ny, nz = self.nseg
         tol = self.jump_tol if margin is None else float(margin)
+        count_fn = lib.nz_cells_count_round if rounded else lib.nz_cells_count
+        fill_fn = lib.nz_cells_fill_round if rounded else lib.nz_cells_fill
         counts = torch.empty(self.ncell, dtype=torch.int32, device=dev)
-        L.check(lib.nz_cells_count(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, tol, _p(counts),
-                                   _stream()), "nz_cells_count")
+        L.check(count_fn(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, tol, _p(counts), _stream()),
+                "nz_cells_count")
         offsets = torch.empty(self.ncell, dtype=torch.int32, device=dev)
         total = torch.zeros(1, dtype=torch.int32, device=dev)
         L.check(lib.nz_exclusive_scan_i32(_p(counts), _p(offsets), self.ncell, _p(total), _stream()),
@@ -178,8 +185,8 @@ class DeviceSubstrate:
         n_items = int(total.item())  # one host sync: the list length sizes the item array
         items = torch.empty(max(n_items, 1), dtype=torch.int32, device=dev)
         cursor = torch.empty(self.ncell, dtype=torch.int32, device=dev)
-        L.check(lib.nz_cells_fill(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, tol, _p(offsets),
-                                  _p(counts), _p(cursor), _p(items), _stream()), "nz_cells_fill")
+        L.check(fill_fn(_p(self.spheres64), self.S, Lx, Ly, Lz, nx, ny, nz, tol, _p(offsets), _p(counts), _p(cursor),
+                        _p(items), _stream()), "nz_cells_fill")
         if not store:
             return offsets, counts, items, n_items
         self.cell_start, self.cell_count, self.cell_items = offsets, counts, items
@@ -187,14 +194,16 @@ class DeviceSubstrate:
 
     def set_near_margin(self, margin: float | None):
         """Build (or drop, with None) the near lists of the fused walk: the
-        same grid with a smaller membership margin (0 < margin < jump_tol)."""
+        same grid with a smaller membership margin (0 < margin < jump_tol),
+        by the Euclidean test when near_round (nz_cells_count_round), else by
+        the reference's box test."""
         if margin is None:
             self.near_margin, self.near = None, None
             return
         margin = float(margin)
         if not 0.0 < margin < self.jump_tol:
             raise NozomiError(f"near margin {margin} must lie in (0, {self.jump_tol})")
-        st, ct, it, n = self._build_cells(margin, store=False)
+        st, ct, it, n = self._build_cells(margin, store=False, rounded=self.near_round)
         dev = _dev()
         self.near_n = n
         if self.idx_bytes:

@@ -30,6 +30,7 @@ class Tuning:
     by_label: bool = True         # re-bin by (label, bin): a warp's walkers share a structure
     near_margin: float | None = 0.5  # margin of the near lists (None: full lists only)
     lists: str = "index"          # the fused walk's list form: "index" (16/32-bit) or "records"
+    near_shape: str = "round"     # near lists by the Euclidean sphere-to-cell test ("round") or the box test
 
 
 def idx_bytes_for(lists: str):
@@ -43,15 +44,17 @@ def idx_bytes_for(lists: str):
 
 def device_substrate(sub: Substrate, D=2.0, T2=100.0, cell: float = 1.0, nseg=None, D_box=None,
                      jump_tol: float = 1.0, near_margin: float | None = None,
-                     lists: str = "index") -> engine.DeviceSubstrate:
+                     lists: str = "index", near_shape: str = "round") -> engine.DeviceSubstrate:
     nseg = cell_grid(sub.L, cell) if nseg is None else nseg
     ns = sub.nstructures
     Dv = np.full(ns + 1, D, np.float32)
     if D_box is not None:
         Dv[ns] = D_box
     T2v = np.full(ns + 1, T2, np.float32)
+    if near_shape not in ("round", "box"):
+        raise ValueError(f"near-list shape {near_shape!r} is not 'round' or 'box'")
     return engine.DeviceSubstrate(sub.spheres(), ns, sub.L, nseg, Dv, T2v, jump_tol=jump_tol, near_margin=near_margin,
-                                  idx_bytes=idx_bytes_for(lists))
+                                  idx_bytes=idx_bytes_for(lists), near_round=near_shape == "round")
 
 
 class DwiRun:
@@ -175,6 +178,7 @@ def simulate_dwi(sub: Substrate, gwave, dirs, bvalues=None, amplitudes=None, N: 
     if amplitudes is None:
         amplitudes = gwave.amplitude_for_b(bvalues)
     tuning = tuning or Tuning()
-    dsub = device_substrate(sub, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin, lists=tuning.lists)
+    dsub = device_substrate(sub, D=D, T2=T2, cell=tuning.cell, near_margin=tuning.near_margin, lists=tuning.lists,
+                            near_shape=tuning.near_shape)
     run = DwiRun(dsub, gwave, dirs, amplitudes, N, seed=seed, targets=targets, tuning=tuning).prepare()
     return run.walk().signal()

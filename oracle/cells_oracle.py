@@ -83,3 +83,28 @@ def padded_as_lists(K: int, segments: np.ndarray, ncell: int):
     start = (np.arange(ncell, dtype=np.int32) * K).astype(np.int32)
     count = np.full(ncell, K, dtype=np.int32)
     return start, count, np.ascontiguousarray(segments, dtype=np.int32)
+
+
+def cells_round(spheres: np.ndarray, L, nseg, margin: float):
+    """The fused walk's rounded near lists (nz_cells_count_round): the
+    members by the box test with jump_tol = margin, keeping only cells whose
+    box lies within r + margin + 1e-4 of the sphere's centre (Euclidean,
+    float64).  (start, count, items), items ascending within a cell."""
+    spheres = np.asarray(spheres, dtype=np.float64)
+    Lx, Ly, Lz = (float(v) for v in L)
+    nx, ny, nz = nseg
+    st, ct, it = cells_members(spheres, L, nseg, margin)
+    dL = (Lx / nx, Ly / ny, Lz / nz)
+    keep = []
+    for c in range(nx * ny * nz):
+        n, m, p = c % nx, (c // nx) % ny, c // (nx * ny)
+        s = it[st[c]:st[c] + ct[c]]
+        lo = np.array([n * dL[0] - Lx / 2, m * dL[1] - Ly / 2, p * dL[2] - Lz / 2])
+        hi = lo + np.array(dL)
+        e = np.maximum(np.maximum(lo[:, None] - spheres[:3, s], 0.0), spheres[:3, s] - hi[:, None])
+        R = spheres[3, s] + margin + 1e-4
+        keep.append(s[(e * e).sum(axis=0) <= R * R])
+    count = np.array([len(x) for x in keep], dtype=np.int32)
+    start = np.zeros(nx * ny * nz, dtype=np.int32)
+    start[1:] = np.cumsum(count)[:-1]
+    return start, count, np.concatenate(keep).astype(np.int32)

@@ -505,3 +505,26 @@ def test_index_lists_with_shuffled_sphere_order(eng, idx_bytes):
     np.testing.assert_array_equal(wk.phi.cpu().numpy(), phi)
     np.testing.assert_array_equal(wk.label.cpu().numpy(), r["label"])
     np.testing.assert_array_equal(wk.flags.cpu().numpy(), r["flags"])
+
+
+def test_rounded_near_lists_match_oracle(eng):
+    """The near lists' Euclidean test on the device (nz_cells_count_round /
+    nz_cells_fill_round) against the numpy restatement, list for list; each
+    a subset of the box test's lists with the same margin, and smaller."""
+    from oracle.cells_oracle import cells_round
+    from nozomi_b200.substrates import axon_bundle, cell_grid
+    sub = axon_bundle(25, seed=4)
+    sph, L3 = sub.spheres(), sub.L
+    nseg = cell_grid(L3, 0.5)
+    ns = sub.nstructures
+    for margin in (0.3, 0.5):
+        d = eng.DeviceSubstrate(sph, ns, L3, nseg, np.full(ns + 1, 2.0), np.full(ns + 1, 100.0), near_margin=margin)
+        box = eng.DeviceSubstrate(sph, ns, L3, nseg, np.full(ns + 1, 2.0), np.full(ns + 1, 100.0),
+                                  near_margin=margin, near_round=False)
+        st, ct, it, n = d.near[0].cpu().numpy(), d.near[1].cpu().numpy(), d.near[2].cpu().numpy(), d.near_n
+        rst, rct, rit = cells_round(sph, L3, nseg, margin)
+        np.testing.assert_array_equal(ct, rct)
+        np.testing.assert_array_equal(st, rst)
+        np.testing.assert_array_equal(it[:n], rit)
+        bct = box.near[1].cpu().numpy()
+        assert np.all(ct <= bct) and ct.sum() < 0.9 * bct.sum()
