@@ -67,9 +67,11 @@ BATCH_WORKLOAD = ("batched mixed workload: {jobs} substrates of 10-500 beaded ax
                   "2000-8000 steps at dt=5 us (PGSE delta=te/3, Delta=2te/3), 6-60 directions, b={{0,1,2,3}} "
                   "ms/um^2, seed 4; all jobs in persistent work-queue launches under one CUDA graph")
 
-# The fused walk's source files: the instruction and DRAM counts below hold
-# for the kernel built from exactly these sources (sha1 of their bytes).
-KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.cuh", "nozomi_b200/csrc/kernels.cuh")
+# The sources the instruction and DRAM counts below depend on: the fused
+# walk's kernel and the construction of the lists it scans (sha1 of their
+# bytes).
+KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.cuh", "nozomi_b200/csrc/kernels.cuh",
+                  "nozomi_b200/csrc/cells.cu", "nozomi_b200/engine.py", "nozomi_b200/simulate.py")
 
 # Per workload, from one ncu capture of walk_fused_kernel (--set full,
 # --clock-control none) on a small case of that workload: warp instructions
