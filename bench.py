@@ -79,16 +79,19 @@ KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.
 # dram__bytes_write.sum) of the captured launch, divided by the walker-steps
 # that launch ran; kernel_sha: the sources' hash at capture.
 PROFILED = {
-    "packed": {"kernel_sha": "9ea3545037c04741", "warp_inst_per_walker_step": 64.591,
-               "dram_bytes_per_walker_step": 1.1100,
+    "packed": {"kernel_sha": "f3d2202768accf96", "warp_inst_per_walker_step": 58.856,
+               "dram_bytes_per_walker_step": 0.9960,
+               "shape": {"cell": 0.5, "near_margin": 0.5, "coarsen": 8, "threads": 128},
                "capture": "walk_fused_kernel<PHI, idx16> launch 3 of `python bench.py --workload packed --walkers "
                           "1000000 --steps-per-launch 200 --steps 1 --warmup 1 --no-cpu-baseline --e2e-steps 0` "
-                          "(200,000,000 walker-steps): 12,918,262,538 warp instructions, 222.0 MB DRAM"},
-    "batched": {"kernel_sha": "9ea3545037c04741", "warp_inst_per_walker_step": 49.074,
-                "dram_bytes_per_walker_step": 0.6649,
+                          "(200,000,000 walker-steps): 11,771,258,482 warp instructions, 199.2 MB DRAM"},
+    "batched": {"kernel_sha": "f3d2202768accf96", "warp_inst_per_walker_step": 43.418,
+                "dram_bytes_per_walker_step": 0.2360,
+                "shape": {"cell": 1.0, "near_margin": 0.5, "coarsen": 4, "threads": 256},
                 "capture": "walk_fused_kernel<PHI, idx16> launch 2 of `python bench.py --walker-scale 0.1 --steps 1 "
-                           "--warmup 1 --no-serving --no-plain --no-cpu-baseline --e2e-steps 0` (64 jobs, "
-                           "787,000,000 walker-steps): 38,621,089,270 warp instructions, 523.3 MB DRAM"},
+                           "--warmup 1 --no-serving --no-plain --no-cpu-baseline --e2e-steps 0 --no-autotune --cell 1.0 "
+                           "--coarsen 4 --steps-per-launch 2000 --threads 256` (64 jobs, 2,407,477,000 walker-steps): "
+                           "104,527,801,690 warp instructions, 568.1 MB DRAM"},
 }
 
 
@@ -153,14 +156,19 @@ def load_peaks():
 
 
 def rooflines(workload: str, kernel_ws_s: float, ws_per_launch: float, launch_ms: float, state_bytes: float,
-              clk, sms: int, fp32_peak_tflops: float, f_alg: float | None, work=None):
+              clk, sms: int, fp32_peak_tflops: float, f_alg: float | None, work=None, shape: dict | None = None):
     """The dominant kernel's rooflines: issue (the binding one), FP32 and HBM.
     kernel_ws_s: its walker-steps per second of kernel time; ws_per_launch:
     walker-steps of an average launch; state_bytes: algorithmic bytes of an
-    average launch (walker state in and out)."""
+    average launch (walker state in and out); shape: the line's launch shape,
+    compared with the one the counts were captured at (the instructions per
+    walker-step depend on the cell size and the near margin)."""
     prof = PROFILED.get(workload, {})
     sha = kernel_sha()
     stale = prof.get("kernel_sha") != sha
+    shape_ok = None
+    if shape is not None and prof.get("shape"):
+        shape_ok = all(shape.get(k) == v for k, v in prof["shape"].items())
     peaks, src = load_peaks()
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
@@ -177,7 +185,7 @@ def rooflines(workload: str, kernel_ws_s: float, ws_per_launch: float, launch_ms
                                     "average launch here",
                  "peak_source": f"{sms} SMs x 4 issue slots x median SM clock under load ({mhz:.0f} MHz)",
                  "counts_kernel_sha": prof.get("kernel_sha"), "kernel_sha": sha, "stale": stale,
-                 "capture": prof.get("capture")}
+                 "counts_shape": prof.get("shape"), "shape_matches": shape_ok, "capture": prof.get("capture")}
     fp32 = None
     if f_alg is not None:
         ach = kernel_ws_s * f_alg / 1e12
@@ -651,8 +659,9 @@ def run_packed(args):
         if wk is not None:
             F_alg = 10 * wk["spheres_in_reach"] + 36 * wk["solves_in_reach"] + 6 * dirs.shape[1]
         # walker state read and written once per launch (4 x float4 each way)
-        roof_issue, roof_fp32, roof_hbm = rooflines("packed", kernel_ws_s, per_launch_ws, walk_launch_ms, N * 128,
-                                                    clk, sms, fp32_peak_tflops, F_alg, wk)
+        roof_issue, roof_fp32, roof_hbm = rooflines(
+            "packed", kernel_ws_s, per_launch_ws, walk_launch_ms, N * 128, clk, sms, fp32_peak_tflops, F_alg, wk,
+            shape={"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": 128})
         line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -951,8 +960,9 @@ def run_batched(args):
     launch_ms = walk_ms / max(len(ev), 1)
     ws_launch = sum(chunk_ws) / max(len(chunk_ws), 1)
     state_bytes = 128 * sum(c["sort_walkers"] for c in run.chunks) / max(len(run.chunks), 1)
-    roof_issue, roof_fp32, roof_hbm = rooflines("batched", kernel_ws_s, ws_launch, launch_ms, state_bytes, clk, sms,
-                                                fp32_peak_tflops, F_alg, wk_all)
+    roof_issue, roof_fp32, roof_hbm = rooflines(
+        "batched", kernel_ws_s, ws_launch, launch_ms, state_bytes, clk, sms, fp32_peak_tflops, F_alg, wk_all,
+        shape={"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": threads})
     line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32",
