@@ -173,6 +173,8 @@ def step_tables(gwave) -> tuple[np.ndarray, np.ndarray]:
     if wave.size > 1:
         area[1:] = np.cumsum((wave[1:] + wave[:-1]) / 2.0)
     area = area * dt
-    G = np.array([np.float32(wave[n] * dt * 267.5 / 10000) for n in range(wave.size)], np.float32)
-    Ga = np.array([np.float32(area[n] * 267.7 / 10000) for n in range(wave.size)], np.float32)
+    # element by element the same float64 operations, in the same order, as
+    # the reference's scalar expressions, then one rounding to float32
+    G = (((wave * dt) * 267.5) / 10000).astype(np.float32)
+    Ga = ((area * 267.7) / 10000).astype(np.float32)
     return G, Ga
