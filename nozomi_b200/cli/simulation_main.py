@@ -30,12 +30,19 @@ import torch
 from .. import _lib as L
 from ..diffsim3d import DiffSim3d
 from ..geometry import SimGeometry3D, Structure3D
-from ..substrates import bound_z, load_pickle, split_fibers
+from ..substrates import ingest_on_device, load_pickle
 
 
 def build_geometry(substrate_file, D, T2=100, rho=1):
+    """The driver's ingestion (simulation_main.py:37-54): the pickle's matrix
+    split into fibres at z == L/2 and z-padded from each fibre's partner,
+    done on the GPU (substrates.ingest_on_device, bit-identical to the
+    reference's split_matrix_to_list + createBoundaryZ), then one structure
+    per fibre."""
     arr, L_box, box = load_pickle(substrate_file)
-    fibers = bound_z(split_fibers(arr, L_box), box[2])
+    rows, _, lengths = ingest_on_device(arr, L_box, box[2])
+    r = rows.cpu().numpy()
+    fibers = np.split(r, np.cumsum(lengths)[:-1]) if len(lengths) else []
     sg3 = SimGeometry3D(box[0], box[1], box[2], D, T2, rho)
     for f in fibers:
         sg3.add_structure(Structure3D(f[:, 0], f[:, 1], f[:, 2], f[:, 3], D, T2, rho))
