@@ -69,9 +69,10 @@ BATCH_WORKLOAD = ("batched mixed workload: {jobs} substrates of 10-500 beaded ax
 
 # The sources the instruction and DRAM counts below depend on: the fused
 # walk's kernel and the construction of the lists it scans (sha1 of their
-# bytes).
+# bytes).  The launch shape and the list form, chosen by the host code, are
+# recorded beside the counts instead.
 KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.cuh", "nozomi_b200/csrc/kernels.cuh",
-                  "nozomi_b200/csrc/cells.cu", "nozomi_b200/engine.py", "nozomi_b200/simulate.py")
+                  "nozomi_b200/csrc/cells.cu", "nozomi_b200/engine.py")
 
 # Per workload, from one ncu capture of walk_fused_kernel (--set full,
 # --clock-control none) on a small case of that workload: warp instructions
@@ -79,15 +80,17 @@ KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.
 # dram__bytes_write.sum) of the captured launch, divided by the walker-steps
 # that launch ran; kernel_sha: the sources' hash at capture.
 PROFILED = {
-    "packed": {"kernel_sha": "f3d2202768accf96", "warp_inst_per_walker_step": 58.856,
+    "packed": {"kernel_sha": "a5f6d060ecad94bb", "warp_inst_per_walker_step": 58.856,
                "dram_bytes_per_walker_step": 0.9960,
-               "shape": {"cell": 0.5, "near_margin": 0.5, "coarsen": 8, "threads": 128},
+               "shape": {"cell": 0.5, "near_margin": 0.5, "coarsen": 8, "threads": 128, "lists": "index",
+                         "near_shape": "round"},
                "capture": "walk_fused_kernel<PHI, idx16> launch 3 of `python bench.py --workload packed --walkers "
                           "1000000 --steps-per-launch 200 --steps 1 --warmup 1 --no-cpu-baseline --e2e-steps 0` "
                           "(200,000,000 walker-steps): 11,771,258,482 warp instructions, 199.2 MB DRAM"},
-    "batched": {"kernel_sha": "f3d2202768accf96", "warp_inst_per_walker_step": 43.418,
+    "batched": {"kernel_sha": "a5f6d060ecad94bb", "warp_inst_per_walker_step": 43.418,
                 "dram_bytes_per_walker_step": 0.2360,
-                "shape": {"cell": 1.0, "near_margin": 0.5, "coarsen": 4, "threads": 256},
+                "shape": {"cell": 1.0, "near_margin": 0.5, "coarsen": 4, "threads": 256, "lists": "index",
+                          "near_shape": "round"},
                 "capture": "walk_fused_kernel<PHI, idx16> launch 2 of `python bench.py --walker-scale 0.1 --steps 1 "
                            "--warmup 1 --no-serving --no-plain --no-cpu-baseline --e2e-steps 0 --no-autotune --cell 1.0 "
                            "--coarsen 4 --steps-per-launch 2000 --threads 256` (64 jobs, 2,407,477,000 walker-steps): "
@@ -613,9 +616,12 @@ def run_packed(args):
     S = sig.cpu().numpy()
     S = (S[0] + 1j * S[1]) / (N * world)
 
-    # end to end with host buffers: positions copied from pinned host memory
-    # into the graph's input, the step replayed, the signal copied back
+    # end to end through the public call with host buffers: the shard's
+    # prepare() copies the positions and labels from pinned host memory,
+    # walk() launches the re-bins and fused walks eagerly, signal_sums()
+    # reduces (and all-reduces over ranks); the sums are copied back
     x_host = x0.cpu().pin_memory()
+    lab_host = lab0.cpu().pin_memory()
     e2e_ms = 0.0
     out_bytes = 0
     host = torch.empty_like(sig_static, device="cpu").pin_memory()
@@ -623,10 +629,8 @@ def run_packed(args):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        x0.copy_(x_host, non_blocking=True)
-        graph.replay()
-        reduce_sums(sig_static)
-        host.copy_(sig_static, non_blocking=True)
+        out = shard.prepare(x_host, lab_host).walk().signal_sums()
+        host.copy_(out, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize()
         out_bytes = host.numel() * host.element_size()
@@ -661,7 +665,8 @@ def run_packed(args):
         # walker state read and written once per launch (4 x float4 each way)
         roof_issue, roof_fp32, roof_hbm = rooflines(
             "packed", kernel_ws_s, per_launch_ws, walk_launch_ms, N * 128, clk, sms, fp32_peak_tflops, F_alg, wk,
-            shape={"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": 128})
+            shape={"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": 128,
+                   "lists": tuning.lists, "near_shape": tuning.near_shape})
         line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -679,8 +684,10 @@ def run_packed(args):
                                           "one all-reduce of the signal sums per step"},
                 "e2e": None if e2e_value is None else {
                     "value": e2e_value, "unit": "walker-steps/s",
-                    "h2d_bytes_per_step": int(x_host.numel() * x_host.element_size()),
-                    "d2h_bytes_per_step": int(out_bytes)},
+                    "h2d_bytes_per_step": int(x_host.numel() * x_host.element_size()
+                                              + lab_host.numel() * lab_host.element_size()),
+                    "d2h_bytes_per_step": int(out_bytes),
+                    "call": "ShardedDwiRun.prepare(host positions, labels).walk().signal_sums(), eager"},
                 "gpu_launches": launches_per_step * args.steps,
                 "kernel": {"name": "walk_fused_kernel", "launches": n_walk, "avg_launch_ms": walk_launch_ms,
                            "walker_steps_per_launch": per_launch_ws, "kernel_walker_steps_per_s": kernel_ws_s,
@@ -962,7 +969,8 @@ def run_batched(args):
     state_bytes = 128 * sum(c["sort_walkers"] for c in run.chunks) / max(len(run.chunks), 1)
     roof_issue, roof_fp32, roof_hbm = rooflines(
         "batched", kernel_ws_s, ws_launch, launch_ms, state_bytes, clk, sms, fp32_peak_tflops, F_alg, wk_all,
-        shape={"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": threads})
+        shape={"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": threads,
+               "lists": tuning.lists, "near_shape": tuning.near_shape})
     line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32",

@@ -92,16 +92,33 @@ class DwiRun:
             return self.positions, None
         return engine.seed(self.sub, self.targets, self.N, key=self.seed ^ 0x5EED, id0=self.id0)
 
-    def prepare(self, positions: torch.Tensor | None = None, labels: torch.Tensor | None = None):
+    def prepare(self, positions=None, labels=None):
+        """Walker state from positions [3, N] and labels [N] (seeded on the
+        device when None).  Host arrays (numpy or CPU tensors) are copied to
+        the current GPU on the current stream, asynchronously when they are
+        pinned; the caller keeps them unchanged until the stream has passed
+        the copy."""
         if positions is None:
             positions, labels = self.initial_positions()
-        x = positions
+        dev = torch.device("cuda", torch.cuda.current_device())
+        x = torch.as_tensor(positions)
+        if x.device != dev or x.dtype != torch.float32:
+            x = x.to(dev, torch.float32, non_blocking=True)
+        if x.dim() != 2 or x.shape[0] != 3:
+            raise TypeError("positions must be a 3 x N array")
         N = x.shape[1]
-        lab = labels if labels is not None else torch.full((N,), -1, dtype=torch.int32, device=x.device)
-        wk = engine.Walkers(x, x.clone(), phi=torch.zeros((6, N), device=x.device), label=lab)
+        if labels is None:
+            lab = torch.full((N,), -1, dtype=torch.int32, device=dev)
+        else:
+            lab = torch.as_tensor(labels)
+            if lab.device != dev or lab.dtype != torch.int32:
+                lab = lab.to(dev, torch.int32, non_blocking=True)
+            if lab.numel() != N:
+                raise TypeError("labels need one entry per walker")
+        wk = engine.Walkers(x.contiguous(), x.clone(), phi=torch.zeros((6, N), device=dev), label=lab.contiguous())
         ids = None
         if self.id0:
-            ids = torch.arange(self.id0, self.id0 + N, dtype=torch.int64, device=x.device).to(torch.int32)
+            ids = torch.arange(self.id0, self.id0 + N, dtype=torch.int64, device=dev).to(torch.int32)
         self.state = engine.FusedState.from_walkers(wk, ids)
         self.spare = engine.FusedState(N)
         self.launches = 1 if N else 0  # library kernels since prepare: the pack

@@ -120,3 +120,13 @@ def test_roofline_counts_are_tied_to_the_kernel_source():
     finally:
         bench.PROFILED["batched"].clear()
         bench.PROFILED["batched"].update(saved)
+
+
+def test_committed_counts_match_the_committed_kernel():
+    """The instruction and DRAM counts the bench line uses were captured on
+    the kernel and list sources in the tree (a kernel change needs a new
+    capture), and on the default list form."""
+    import bench
+    for name, prof in bench.PROFILED.items():
+        assert prof["kernel_sha"] == bench.kernel_sha(), name
+        assert prof["shape"]["lists"] == "index" and prof["shape"]["near_shape"] == "round", name

@@ -183,6 +183,36 @@ def test_sharded_gpu_equals_unsharded():
         np.testing.assert_allclose((sums[0] + 1j * sums[1]) / N, ref_sig, rtol=0, atol=1e-12)
 
 
+@pytest.mark.gpu
+def test_prepare_from_host_buffers_equals_device_buffers():
+    """prepare() given the seeded positions and labels as pinned host tensors
+    and as numpy arrays (the end-to-end call's inputs) walks to the same
+    positions and sums, bit for bit, as given the device tensors."""
+    import torch
+    from nozomi_b200.shard import ShardedDwiRun
+    from nozomi_b200.simulate import Tuning, device_substrate
+    from nozomi_b200.substrates import axon_bundle
+    from nozomi_b200.workloads import pgse, unit_directions
+    sub = axon_bundle(12, seed=5)
+    tuning = Tuning(steps_per_launch=150)
+    dsub = device_substrate(sub, D=2.0, cell=tuning.cell, near_margin=tuning.near_margin)
+    gw = pgse(400)
+    dirs = unit_directions(np.random.default_rng(2), 6)
+    amps = gw.amplitude_for_b([0.0, 1.0, 3.0])
+    sh = ShardedDwiRun(dsub, gw, dirs, amps, 8_193, seed=7, rank=1, world=2, tuning=tuning)
+    x0, lab0 = sh.run.initial_positions()
+    ref = sh.prepare(x0, lab0).walk().local_sums().cpu().numpy()
+    ref_pos = sh.run.walkers().spins.cpu().numpy()
+    for x, lab in ((x0.cpu().pin_memory(), lab0.cpu().pin_memory()), (x0.cpu().numpy(), lab0.cpu().numpy())):
+        got = sh.prepare(x, lab).walk().local_sums().cpu().numpy()
+        np.testing.assert_array_equal(got, ref)
+        np.testing.assert_array_equal(sh.run.walkers().spins.cpu().numpy(), ref_pos)
+    with pytest.raises(TypeError):
+        sh.prepare(x0.cpu()[:2], lab0.cpu())
+    with pytest.raises(TypeError):
+        sh.prepare(x0.cpu(), lab0.cpu()[:-1])
+
+
 def test_oracle_seed_range_is_a_slice_of_the_full_seeding():
     """Walkers [id0, id0 + n) seeded alone are walkers id0.. of one seeding of
     the whole run (positions and labels), the property sharded runs rest on."""
