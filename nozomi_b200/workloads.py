@@ -75,10 +75,13 @@ def calibration_substrate() -> Substrate:
     return s
 
 
+def _bundle_key(n_axons: int, seed: int) -> str:
+    return hashlib.sha1(f"axon_bundle-v2-{n_axons}-{seed}".encode()).hexdigest()[:16]
+
+
 def bundle(n_axons: int, seed: int) -> Substrate:
     CACHE.mkdir(parents=True, exist_ok=True)
-    key = hashlib.sha1(f"axon_bundle-v2-{n_axons}-{seed}".encode()).hexdigest()[:16]
-    path = CACHE / f"bundle_{key}.pkl"
+    path = CACHE / f"bundle_{_bundle_key(n_axons, seed)}.pkl"
     if path.exists():
         with open(path, "rb") as f:
             return pickle.load(f)
@@ -123,12 +126,18 @@ class Request:
 
 def request_stream(rate: float, duration: float, seed: int = 5, reuse: float = 0.7, axons=(10, 500),
                    walkers=(1e4, 5e5), steps=(2000, 8000), ndirs=(6, 60), bmax: float = 3.0,
-                   max_requests: int | None = None) -> list:
+                   max_requests: int | None = None, workers: int | None = None) -> list:
+    """Requests of a Poisson stream at `rate` per second over `duration`
+    seconds (at most max_requests).  A request reuses an earlier request's
+    substrate with probability `reuse`; requests of one substrate share one
+    Substrate object.  Substrates not yet in the disk cache are generated
+    first, by `workers` processes (default: up to 16 when more than 8 are
+    missing); the stream is the same whatever the number of workers."""
     rng = np.random.default_rng(seed)
-    t, out, seen = 0.0, [], []
+    t, drawn, seen = 0.0, [], []
     while True:
         t += rng.exponential(1.0 / rate)
-        if t > duration or (max_requests is not None and len(out) >= max_requests):
+        if t > duration or (max_requests is not None and len(drawn) >= max_requests):
             break
         if seen and rng.uniform() < reuse:
             na, sseed = seen[int(rng.integers(len(seen)))]
@@ -138,9 +147,33 @@ def request_stream(rate: float, duration: float, seed: int = 5, reuse: float = 0
         N = int(max(1000, round(np.exp(rng.uniform(np.log(walkers[0]), np.log(walkers[1]))) / 1000) * 1000))
         nst = int(rng.integers(steps[0], steps[1] + 1))
         nd = int(rng.integers(ndirs[0], ndirs[1] + 1))
-        gw = pgse(nst)
         b = np.linspace(0.0, rng.uniform(1.0, bmax), 4)
-        spec = JobSpec(bundle(na, sseed), gw, unit_directions(rng, nd), gw.amplitude_for_b(b), N,
-                       seed=int(rng.integers(1 << 31)), key=("bundle", na, sseed))
+        dirs = unit_directions(rng, nd)
+        drawn.append((t, na, sseed, N, nst, dirs, b, int(rng.integers(1 << 31))))
+    subs = bundles(seen, workers)
+    out = []
+    for t, na, sseed, N, nst, dirs, b, rseed in drawn:
+        gw = pgse(nst)
+        spec = JobSpec(subs[(na, sseed)], gw, dirs, gw.amplitude_for_b(b), N, seed=rseed, key=("bundle", na, sseed))
         out.append(Request(t, spec))
     return out
+
+
+def _bundle_args(args):
+    return bundle(*args)
+
+
+def bundles(keys, workers: int | None = None) -> dict:
+    """{(n_axons, seed): bundle(n_axons, seed)} for every key; the ones not
+    in the disk cache are generated in `workers` spawned processes when
+    there are more than 8 of them (workers None: up to 16)."""
+    keys = list(dict.fromkeys(keys))
+    missing = [k for k in keys if not (CACHE / f"bundle_{_bundle_key(*k)}.pkl").exists()]
+    if workers is None:
+        workers = min(16, os.cpu_count() or 1) if len(missing) > 8 else 1
+    if workers > 1 and missing:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            list(ex.map(_bundle_args, missing, chunksize=4))  # written to the disk cache
+    return {k: bundle(*k) for k in keys}

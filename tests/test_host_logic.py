@@ -221,3 +221,24 @@ def test_record_order_of_the_index_lists():
     rec4, rec_sid, sid_start, perm = record_order(np.zeros((5, 0)), 0)
     assert rec4.shape == (1, 4) and rec_sid.shape == (1,) and perm.shape == (1,)
     np.testing.assert_array_equal(sid_start, [0, 0])
+
+
+def test_stream_substrates_generated_in_workers_equal_in_process(tmp_path, monkeypatch):
+    """Substrates generated by spawned worker processes (then read back from
+    the disk cache) equal the ones generated in this process; requests of one
+    substrate share one object."""
+    from nozomi_b200 import workloads
+    keys = [(10, 11), (11, 12), (10, 13), (10, 11)]
+    monkeypatch.setenv("NOZOMI_B200_CACHE", str(tmp_path / "w"))
+    monkeypatch.setattr(workloads, "CACHE", tmp_path / "w")
+    par = workloads.bundles(keys, workers=2)
+    monkeypatch.setenv("NOZOMI_B200_CACHE", str(tmp_path / "s"))
+    monkeypatch.setattr(workloads, "CACHE", tmp_path / "s")
+    seq = workloads.bundles(keys, workers=1)
+    assert sorted(par) == sorted(seq) == sorted(set(keys))
+    for k in seq:
+        np.testing.assert_array_equal(par[k].spheres(), seq[k].spheres())
+    reqs = workloads.request_stream(40.0, 2.0, seed=3, axons=(10, 11), walkers=(1e4, 2e4), steps=(2000, 2100))
+    by_key = {}
+    for r in reqs:
+        assert by_key.setdefault(r.spec.key, r.spec.substrate) is r.spec.substrate
