@@ -62,7 +62,7 @@ sys.path.insert(0, str(ROOT))
 WORKLOAD = ("packed substrate: 200 beaded axons x 100 spheres (lognormal r0 1.0/0.3 um, bead amplitude "
             "U[0.2,0.5]), periodic 40x40x80 um box, 1e6 walkers/GPU over intra+extra space, D=2.0 um^2/ms, "
             "PGSE delta=10 Delta=20 te=30 ms at dt=5 us (6000 steps), 30 directions x b={0,1,2,3} ms/um^2")
-BATCH_WORKLOAD = ("batched mixed workload: {jobs} substrates of 10-500 beaded axons (40 spheres at 1 um, radii "
+BATCH_WORKLOAD = ("batched mixed workload: {jobs} substrates of {a0}-{a1} beaded axons (40 spheres at 1 um, radii "
                   "U[0.5,1.5], z-periodic, packed at area fraction 0.35), walkers log-uniform 1e4-1e6 (x{scale}), "
                   "2000-8000 steps at dt=5 us (PGSE delta=te/3, Delta=2te/3), 6-60 directions, b={{0,1,2,3}} "
                   "ms/um^2, seed 4; all jobs in persistent work-queue launches under one CUDA graph")
@@ -80,21 +80,21 @@ KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.
 # dram__bytes_write.sum) of the captured launch, divided by the walker-steps
 # that launch ran; kernel_sha: the sources' hash at capture.
 PROFILED = {
-    "packed": {"kernel_sha": "a5f6d060ecad94bb", "warp_inst_per_walker_step": 58.856,
-               "dram_bytes_per_walker_step": 0.9960,
+    "packed": {"kernel_sha": "42d7c0b4116230f5", "warp_inst_per_walker_step": 58.857,
+               "dram_bytes_per_walker_step": 0.9932,
                "shape": {"cell": 0.5, "near_margin": 0.5, "coarsen": 8, "threads": 128, "lists": "index",
                          "near_shape": "round"},
                "capture": "walk_fused_kernel<PHI, idx16> launch 3 of `python bench.py --workload packed --walkers "
                           "1000000 --steps-per-launch 200 --steps 1 --warmup 1 --no-cpu-baseline --e2e-steps 0` "
-                          "(200,000,000 walker-steps): 11,771,258,482 warp instructions, 199.2 MB DRAM"},
-    "batched": {"kernel_sha": "a5f6d060ecad94bb", "warp_inst_per_walker_step": 43.418,
+                          "(200,000,000 walker-steps): 11,771,485,495 warp instructions, 198.6 MB DRAM"},
+    "batched": {"kernel_sha": "42d7c0b4116230f5", "warp_inst_per_walker_step": 43.418,
                 "dram_bytes_per_walker_step": 0.2360,
                 "shape": {"cell": 1.0, "near_margin": 0.5, "coarsen": 4, "threads": 256, "lists": "index",
                           "near_shape": "round"},
                 "capture": "walk_fused_kernel<PHI, idx16> launch 2 of `python bench.py --walker-scale 0.1 --steps 1 "
                            "--warmup 1 --no-serving --no-plain --no-cpu-baseline --e2e-steps 0 --no-autotune --cell 1.0 "
                            "--coarsen 4 --steps-per-launch 2000 --threads 256` (64 jobs, 2,407,477,000 walker-steps): "
-                           "104,527,801,690 warp instructions, 568.1 MB DRAM"},
+                           "104,528,520,791 warp instructions, 568.2 MB DRAM"},
 }
 
 
@@ -134,6 +134,9 @@ def parse(argv=None):
     ap.add_argument("--lists", default=None, choices=["index", "records"],
                     help="the fused walk's list form: index (16/32-bit entries into one record array) or records "
                          "(per-entry sphere records)")
+    ap.add_argument("--stage", type=int, default=None,
+                    help="batched: records per CTA staged in shared memory by a bulk copy (nz_walk_batch_staged; "
+                         "0: none, records read through L1/L2)")
     ap.add_argument("--narrow-walkers", type=float, default=5e5, help="narrow: walkers")
     ap.add_argument("--narrow-ms", type=float, default=100.0, help="narrow: simulated time, ms")
     ap.add_argument("--serve", default="5:30,20:10",
@@ -144,6 +147,8 @@ def parse(argv=None):
     ap.add_argument("--max-requests", type=int, default=None, help="serving: requests per rate at most")
     ap.add_argument("--jobs", type=int, default=64, help="batched: number of substrates")
     ap.add_argument("--walker-scale", type=float, default=1.0, help="batched: scale of the walker counts")
+    ap.add_argument("--axons", type=lambda v: [int(a) for a in v.split(",")], default=[10, 500],
+                    help="batched: range of axon counts per substrate, lo,hi")
     ap.add_argument("--threads", type=int, default=128, help="batched: walkers per CTA")
     ap.add_argument("--plain-every", type=int, default=4, help="batched: time the plain path on every k-th job")
     ap.add_argument("--no-plain", action="store_true", help="batched: skip the plain-path comparison")
@@ -404,7 +409,8 @@ def run_reference(args):
         value, cores, sample = port_sample(cases, args.cpu_seconds / 2, steps=args.steps, warmup=args.warmup)
         ms_step = None  # samples of differing walker counts: no common step time
         kind, how = "port", f"oracle/walk_oracle.c, the C restatement of the kernel, OpenMP over walkers ({e})"
-    wl = WORKLOAD if workload == "packed" else BATCH_WORKLOAD.format(jobs=args.jobs, scale=args.walker_scale)
+    wl = WORKLOAD if workload == "packed" else BATCH_WORKLOAD.format(jobs=args.jobs, scale=args.walker_scale,
+                                                                       a0=args.axons[0], a1=args.axons[1])
     line = {"impl": "reference", "metric": "walker-steps/s", "value": value, "unit": "walker-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak" if workload == "packed" else "strong",
@@ -723,6 +729,8 @@ def _tuning_from_args(args, base):
         base.lists = args.lists
     if args.near_shape:
         base.near_shape = args.near_shape
+    if args.stage is not None:
+        base.stage = args.stage
     return base
 
 
@@ -801,7 +809,7 @@ def run_batched(args):
         init_process_group("nccl", timeout_s=180)
     engine.require_cuda()
     t0 = time.perf_counter()
-    all_specs = mixed_specs(seed=4, n_jobs=args.jobs, walker_scale=args.walker_scale)
+    all_specs = mixed_specs(seed=4, n_jobs=args.jobs, walker_scale=args.walker_scale, axons=tuple(args.axons))
     gen_s = time.perf_counter() - t0
     # over several GPUs the jobs shard whole, longest first onto the least
     # loaded rank; no data crosses ranks (strong scaling of a fixed batch)
@@ -898,13 +906,13 @@ def run_batched(args):
     value = ws * args.steps / (ms * 1e-3)
     e2e_value = ws * args.e2e_steps / (e2e_ms * 1e-3) if args.e2e_steps else None
     kernel_ws_s = sum(chunk_ws) / (walk_ms * 1e-3)
-    wl = BATCH_WORKLOAD.format(jobs=len(all_specs), scale=args.walker_scale)
+    wl = BATCH_WORKLOAD.format(jobs=len(all_specs), scale=args.walker_scale, a0=args.axons[0], a1=args.axons[1])
     config = {"workload": wl, "jobs": len(all_specs), "walker_steps_per_step": ws,
               "walkers": sum(sp.N for sp in all_specs), "threads": threads,
               "steps_per_launch": tuning.steps_per_launch, "near_margin_um": tuning.near_margin,
               "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen, "rebin_by_label": tuning.by_label,
-              "lists": tuning.lists, "near_shape": tuning.near_shape, "persistent_grid": run.grid,
-              "chunks": len(run.chunks),
+              "lists": tuning.lists, "near_shape": tuning.near_shape, "stage_records": tuning.stage,
+              "persistent_grid": run.grid, "chunks": len(run.chunks),
               "l2": "256 MiB flush between timed steps (the inputs, 64 substrates' cell lists and walker "
                     "state, are also larger than L2)",
               "parallelism": (f"jobs sharded whole over {world} GPUs, longest first" if world > 1 else "one GPU")}

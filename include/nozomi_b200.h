@@ -50,6 +50,9 @@ extern "C" {
 #define NZ_FLAG_ITER_CAP 2
 #define NZ_FLAG_UNSEEDED 4
 #define NZ_FLAG_BOUNDS 8    /* bounds-checked build only: an index was out of range (the access was skipped) */
+#define NZ_FLAG_STAGE_TIMEOUT 16 /* nz_walk_batch_staged: the copy of the substrate's records into shared
+                                    memory did not complete in time; the records were read from global memory
+                                    (the walk's result is unchanged) */
 
 /* Box [-L/2, L/2]^3 and uniform cell grid: the reference kernel's template
  * constants Lx..Lz, dLx..dLz, nLx..nLz (sim3d_kernel.cu:17-28). */
@@ -345,6 +348,28 @@ int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_it
 /* CTAs of `threads` walkers of the batched walk in `mode` that fit on one SM
  * (the persistent grid is this times the SM count). */
 int nz_batch_occupancy(int mode, int threads, int* blocks_per_sm);
+
+/* nz_walk_batch with each job's sphere records staged in shared memory: a CTA
+ * whose item belongs to a job of at most stage_records records (S) copies that
+ * job's record array (S x 16 bytes) into its shared memory with one bulk copy
+ * (cp.async.bulk, completing on an mbarrier) and reads every record of the
+ * walk from there; the copy is reused by the CTA's next items of the same
+ * job.  Jobs with more records, or whose record array does not start on a
+ * 16-byte boundary, read global memory as in nz_walk_batch.  Index lists only
+ * (mode carries NZ_LIST_IDX16 or NZ_LIST_IDX32); stage_records in
+ * [0, 12288] (192 KiB per CTA; 0 is nz_walk_batch).  Results are bit-identical
+ * to nz_walk_batch's.  Every wait for a copy is bounded: a copy that does not
+ * complete in time is abandoned, the CTA reads global memory from then on and
+ * its walkers of that item get NZ_FLAG_STAGE_TIMEOUT.  Replaces the same
+ * gather as nz_walk_batch (reference: segmentList[idxSeg*K+n] in
+ * randomWalk3d_phase_multidirr, sim3d_kernel.cu:767-783 and :801-841), with
+ * the records in shared memory instead of L1/L2. */
+int nz_walk_batch_staged(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0,
+                         int step1, int* queue, int grid, int threads, int stage_records, void* stream);
+
+/* nz_batch_occupancy for nz_walk_batch_staged with stage_records records of
+ * shared memory per CTA (index lists only). */
+int nz_batch_occupancy_staged(int mode, int threads, int stage_records, int* blocks_per_sm);
 
 /* ---- walker re-binning: a stable-key counting sort of the packed state by
  * cell, so that the walkers of one CTA share cells.  bins: bin per walker is

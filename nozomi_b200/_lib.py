@@ -20,7 +20,8 @@ LIB_PATH = Path(__file__).resolve().parent / ("libnozomi_b200_debug.so" if DEBUG
 NZ_OK, NZ_ERR_ARG, NZ_ERR_CUDA, NZ_ERR_CAPACITY, NZ_ERR_UNSEEDED = 0, 1, 2, 3, 4
 MODE_SIG, MODE_PHASE, MODE_PHI, MODE_MOMENTS, MODE_TANGENT64 = 1, 2, 4, 8, 16
 LIST_IDX16, LIST_IDX32 = 64, 128  # nz_walk_batch: the jobs' list format (none: per-entry records)
-FLAG_DRAWS_EXHAUSTED, FLAG_ITER_CAP, FLAG_UNSEEDED, FLAG_BOUNDS = 1, 2, 4, 8
+FLAG_DRAWS_EXHAUSTED, FLAG_ITER_CAP, FLAG_UNSEEDED, FLAG_BOUNDS, FLAG_STAGE_TIMEOUT = 1, 2, 4, 8, 16
+MAX_STAGE_RECORDS = 12288  # nz_walk_batch_staged: records a CTA stages in shared memory at most
 FUSED_THREADS = 128       # walkers per CTA / per work item of the fused and batched walks
 MOMENT_STEPS = 256        # steps per launch when the fused walk accumulates moments
 SCAN_SINGLE_KEYS = 32768  # nz_state_sort scans up to this many bins in one kernel, beyond it in three
@@ -106,6 +107,8 @@ SIGNATURES = {
     "nz_walk_fused_moments": (_i, [_P, _P, _i, _f, _P, _P, _i, _i, _P, _P, ctypes.c_size_t, _P, _P]),
     "nz_walk_batch": (_i, [_P, _i, _P, _i, _i, _i, _i, _P, _i, _i, _P]),
     "nz_batch_occupancy": (_i, [_i, _i, _P]),
+    "nz_walk_batch_staged": (_i, [_P, _i, _P, _i, _i, _i, _i, _P, _i, _i, _i, _P]),
+    "nz_batch_occupancy_staged": (_i, [_i, _i, _i, _P]),
     "nz_sort_scratch_bytes": (ctypes.c_size_t, [_i, _i]),
     "nz_state_sort": (_i, [_P, _P, _i, _P, _P, ctypes.c_size_t, _P]),
     "nz_state_sort_keyed": (_i, [_P, _P, _i, _i, _P, _P, ctypes.c_size_t, _P]),

@@ -148,14 +148,34 @@ def list_groups(jobs, active) -> dict:
     return groups
 
 
-def batch_grid(threads: int, lk: int) -> int:
-    """Persistent grid of the batched walk: CTAs resident per SM x SMs."""
+def batch_grid(threads: int, lk: int, stage: int = 0) -> int:
+    """Persistent grid of the batched walk: CTAs resident per SM x SMs
+    (with `stage` records of shared memory per CTA for index lists)."""
     dev = torch.device("cuda", torch.cuda.current_device())
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     occ = ctypes.c_int(0)
-    L.check(L.load().nz_batch_occupancy(L.MODE_PHI | LIST_BITS[lk], int(threads), ctypes.byref(occ)),
-            "nz_batch_occupancy")
+    lib = L.load()
+    if stage and lk:
+        L.check(lib.nz_batch_occupancy_staged(L.MODE_PHI | LIST_BITS[lk], int(threads), int(stage),
+                                              ctypes.byref(occ)), "nz_batch_occupancy_staged")
+    else:
+        L.check(lib.nz_batch_occupancy(L.MODE_PHI | LIST_BITS[lk], int(threads), ctypes.byref(occ)),
+                "nz_batch_occupancy")
     return sms * max(1, occ.value)
+
+
+def launch_batch(table, n_jobs: int, items, lk: int, s0: int, s1: int, queue_ptr: int, grid: int, threads: int,
+                 stage: int, stream) -> None:
+    """One batched walk launch over `items` (list form lk): nz_walk_batch, or
+    nz_walk_batch_staged when `stage` records per CTA are staged (index lists
+    only; record lists are never staged)."""
+    lib = L.load()
+    args = (ctypes.c_void_p(table.data_ptr()), int(n_jobs), ctypes.c_void_p(items.data_ptr()), int(items.shape[0]),
+            L.MODE_PHI | LIST_BITS[lk], int(s0), int(s1), ctypes.c_void_p(queue_ptr), int(grid), int(threads))
+    if stage and lk:
+        L.check(lib.nz_walk_batch_staged(*args, int(stage), stream), "nz_walk_batch_staged")
+    else:
+        L.check(lib.nz_walk_batch(*args, stream), "nz_walk_batch")
 
 
 def _items(jobs, active, threads, s0, k) -> torch.Tensor:
@@ -205,7 +225,8 @@ class BatchRun:
         # and amplitudes above, plus positions given as host arrays and the
         # chunk tables (added by prepare)
         self.h2d_bytes = sum(j["G"].numel() * 8 + j["dirs"].numel() * 4 + j["amps"].numel() * 4 for j in self.jobs)
-        self.grids = {lk: batch_grid(self.threads, lk) for lk in {j["sub"].idx_bytes for j in self.jobs}}
+        self.grids = {lk: batch_grid(self.threads, lk, self.tuning.stage)
+                      for lk in {j["sub"].idx_bytes for j in self.jobs}}
         self.grid = max(self.grids.values())
         self._planned = False
 
@@ -297,11 +318,9 @@ class BatchRun:
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(cs)
             for g, (lk, items) in enumerate(c["launches"]):
-                L.check(lib.nz_walk_batch(ctypes.c_void_p(c["table"].data_ptr()), len(self.jobs),
-                                          ctypes.c_void_p(items.data_ptr()), int(items.shape[0]),
-                                          L.MODE_PHI | LIST_BITS[lk], c["s0"], c["s1"],
-                                          ctypes.c_void_p(self.queue.data_ptr() + 4 * (3 * qi + g)), self.grids[lk],
-                                          self.threads, stream), "nz_walk_batch")
+                launch_batch(c["table"], len(self.jobs), items, lk, c["s0"], c["s1"],
+                             self.queue.data_ptr() + 4 * (3 * qi + g), self.grids[lk], self.threads,
+                             self.tuning.stage, stream)
             if events is not None:
                 e1.record(cs)
                 events.append((e0, e1))

@@ -245,22 +245,41 @@ extern "C" int nz_walk_fused_moments(const nz_substrate* sub, const nz_state* st
   return check_launch("disp_moments_kernel");
 }
 
-extern "C" int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0,
-                             int step1, int* queue, int grid, int threads, void* stream) {
+// nz_walk_batch with stage_records records of shared memory per CTA for
+// staging (0: none).  A job is staged when its record array fits and starts on
+// a 16-byte boundary (the kernel checks; other jobs read global memory).
+static int walk_batch(const char* what, const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode,
+                      int step0, int step1, int* queue, int grid, int threads, int stage_records, void* stream) {
   if (!jobs || n_jobs <= 0 || !items || n_items < 0 || step0 < 0 || step1 < step0 || grid < 0)
-    return set_error(NZ_ERR_ARG, "nz_walk_batch: bad arguments");
+    return set_error(NZ_ERR_ARG, "%s: bad arguments", what);
   if (threads < 32 || threads > kFusedMaxThreads || threads % 32)
-    return set_error(NZ_ERR_ARG, "nz_walk_batch: threads %d not a multiple of 32 in [32, %d]", threads,
-                     kFusedMaxThreads);
-  if (grid > 0 && !queue) return set_error(NZ_ERR_ARG, "nz_walk_batch: a persistent grid needs a queue counter");
-  if (mode & NZ_MODE_MOMENTS) return set_error(NZ_ERR_ARG, "nz_walk_batch: moments are per-substrate (nz_walk_fused)");
+    return set_error(NZ_ERR_ARG, "%s: threads %d not a multiple of 32 in [32, %d]", what, threads, kFusedMaxThreads);
+  if (grid > 0 && !queue) return set_error(NZ_ERR_ARG, "%s: a persistent grid needs a queue counter", what);
+  if (mode & NZ_MODE_MOMENTS) return set_error(NZ_ERR_ARG, "%s: moments are per-substrate (nz_walk_fused)", what);
   const int lk = batch_list_kind(mode);
-  if (lk < 0) return set_error(NZ_ERR_ARG, "nz_walk_batch: both list widths in mode %d", mode);
+  if (lk < 0) return set_error(NZ_ERR_ARG, "%s: both list widths in mode %d", what, mode);
+  if (stage_records < 0 || stage_records > kMaxStageRecords)
+    return set_error(NZ_ERR_ARG, "%s: stage_records %d outside [0, %d]", what, stage_records, kMaxStageRecords);
+  if (stage_records > 0 && lk == 0)
+    return set_error(NZ_ERR_ARG, "%s: records are staged for index lists only (no NZ_LIST_IDX bit in mode)", what);
   if (n_items == 0 || step1 == step0) return NZ_OK;
   const JobDev unused{};
   return launch_fused(mode & ~(NZ_LIST_IDX16 | NZ_LIST_IDX32), lk, unused, jobs, items, n_items, step0, step1,
                       grid > 0 ? queue : nullptr, grid > 0 ? grid : n_items, threads,
-                      static_cast<cudaStream_t>(stream));
+                      static_cast<cudaStream_t>(stream), stage_records);
+}
+
+extern "C" int nz_walk_batch(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode, int step0,
+                             int step1, int* queue, int grid, int threads, void* stream) {
+  return walk_batch("nz_walk_batch", jobs, n_jobs, items, n_items, mode, step0, step1, queue, grid, threads, 0,
+                    stream);
+}
+
+extern "C" int nz_walk_batch_staged(const nz_job* jobs, int n_jobs, const nz_item* items, int n_items, int mode,
+                                    int step0, int step1, int* queue, int grid, int threads, int stage_records,
+                                    void* stream) {
+  return walk_batch("nz_walk_batch_staged", jobs, n_jobs, items, n_items, mode, step0, step1, queue, grid, threads,
+                    stage_records, stream);
 }
 
 extern "C" int nz_batch_occupancy(int mode, int threads, int* blocks_per_sm) {
@@ -268,4 +287,12 @@ extern "C" int nz_batch_occupancy(int mode, int threads, int* blocks_per_sm) {
   if (!blocks_per_sm || threads < 32 || threads > kFusedMaxThreads || lk < 0)
     return set_error(NZ_ERR_ARG, "nz_batch_occupancy: bad arguments");
   return occupancy_fused(mode & ~(NZ_LIST_IDX16 | NZ_LIST_IDX32), lk, threads, blocks_per_sm);
+}
+
+extern "C" int nz_batch_occupancy_staged(int mode, int threads, int stage_records, int* blocks_per_sm) {
+  const int lk = batch_list_kind(mode);
+  if (!blocks_per_sm || threads < 32 || threads > kFusedMaxThreads || lk <= 0 || stage_records < 0 ||
+      stage_records > kMaxStageRecords)
+    return set_error(NZ_ERR_ARG, "nz_batch_occupancy_staged: bad arguments");
+  return occupancy_fused(mode & ~(NZ_LIST_IDX16 | NZ_LIST_IDX32), lk, threads, blocks_per_sm, stage_records);
 }

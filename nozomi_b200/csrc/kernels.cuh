@@ -50,6 +50,8 @@ __global__ void walk_plain_kernel(const PlainArgs a);
 // ---- fused walk (walk_fused.cu) ----
 constexpr int kFusedThreads = 128;     // walkers per CTA of nz_walk_fused
 constexpr int kFusedMaxThreads = 256;  // largest CTA of nz_walk_batch
+constexpr int kMaxStageRecords = 12288;  // records a CTA of the staged batched walk holds in shared memory (192 KiB)
+constexpr size_t kSmemPerSm = 228 * 1024;  // shared memory an SM can give its CTAs (sm_100)
 #ifndef NZ_FUSED_MIN_BLOCKS
 #define NZ_FUSED_MIN_BLOCKS 3
 #endif
@@ -111,8 +113,8 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
                                     const nz_draws& d, int mode, const nz_state& st, double* moments);
 // lk: list kind, 0 (per-entry records), 2 or 4 (index lists of that width)
 int launch_fused(int mode, int lk, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items,
-                 int step0, int step1, int* queue, int grid, int threads, cudaStream_t st);
-int occupancy_fused(int mode, int lk, int threads, int* blocks_per_sm);
+                 int step0, int step1, int* queue, int grid, int threads, cudaStream_t st, int stage_cap = 0);
+int occupancy_fused(int mode, int lk, int threads, int* blocks_per_sm, int stage_cap = 0);
 __global__ void pack_kernel(nz_walkers wk, const uint32_t* ids, nz_state st);
 __global__ void disp_moments_kernel(const float* __restrict__ disp, int N, double* __restrict__ out);
 __global__ void unpack_kernel(nz_state st, nz_walkers wk, int by_id, int* bad);

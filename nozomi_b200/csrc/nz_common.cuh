@@ -21,6 +21,8 @@ enum : int {
   kFlagIterCap = 2,         // a step ended at the 100-iteration cap
   kFlagUnseeded = 4,        // seeding gave up after its round limit
   kFlagBounds = 8,          // bounds-checked build: an index was out of range and its access skipped
+  kFlagStageTimeout = 16,   // staged walk: the record copy into shared memory did not complete in time;
+                            // the walker read its records from global memory instead (results unchanged)
 };
 
 // The bounds-checked build (-DNZ_DEBUG_BOUNDS=1, libnozomi_b200_debug.so):

@@ -35,6 +35,7 @@
 //    regrouped; identical in exact arithmetic);
 //  * draws are counter-based (Philox at walker, step, draw), so a walker's
 //    trajectory does not depend on which thread, CTA or launch runs it.
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 #include "kernels.cuh"
@@ -53,7 +54,10 @@ struct ScanOut {
 // record index outside [0, S) sets oob and reads nothing: the entry becomes
 // a NaN record that is neither near nor containing, with a key that stops
 // nothing.
-template <int LK>
+// The records of a job staged in shared memory (staged batched walk only).
+extern __shared__ __align__(16) float4 s_stage[];
+
+template <int LK, bool SH>
 __device__ __forceinline__ void entry(const void* __restrict__ list, const float4* __restrict__ rec,
                                       const int* __restrict__ sid, int k, bool box, int S, int& oob, int& key,
                                       float4& c) {
@@ -69,7 +73,8 @@ __device__ __forceinline__ void entry(const void* __restrict__ list, const float
       c = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
       return;
     }
-    c = __ldg(rec + key);
+    if constexpr (SH) c = s_stage[key];  // SH: the job's records were copied into s_stage
+    else c = __ldg(rec + key);
   }
 }
 
@@ -80,7 +85,7 @@ __device__ __forceinline__ void entry(const void* __restrict__ list, const float
 // form an entry's structure is compared through its record index: records
 // [lo, hi) are structure L's, so key < hi is "structure <= L" and key < lo
 // "structure < L".
-template <int LK, bool T64>
+template <int LK, bool T64, bool SH>
 __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const float4* __restrict__ rec,
                                           const int* __restrict__ sid, int start, int count, int nstructures,
                                           int lo, int hi, float x, float y, float z, int L, float a, float jx,
@@ -110,7 +115,7 @@ __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const f
 #pragma unroll
       for (int u = 0; u < kScanUnroll; ++u) {
         if (kScanUnroll == 1 || i0 + u < m) {
-          entry<LK>(list, rec, sid, start + base + i0 + u, box, S, oob, key[u], c[u]);
+          entry<LK, SH>(list, rec, sid, start + base + i0 + u, box, S, oob, key[u], c[u]);
         } else {  // past the chunk: a NaN record, never near, stops nothing
           key[u] = -1;
           c[u] = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
@@ -135,7 +140,7 @@ __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const f
       near_mask &= near_mask - 1;
       int key;
       float4 c;
-      entry<LK>(list, rec, sid, start + base + i, box, S, oob, key, c);
+      entry<LK, SH>(list, rec, sid, start + base + i, box, S, oob, key, c);
       const bool below = LK == 0 ? key < L : (box || key < lo);
       const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
       const float d2 = dx * dx + dy * dy + dz * dz;
@@ -159,7 +164,7 @@ __device__ __forceinline__ bool scan_cell(const void* __restrict__ list, const f
 // The reference's label pass (sim3d_kernel.cu:766-785): lowest structure id
 // among the spheres containing the walker, nstructures if none.  In index
 // form the entries ascend by structure, so the first containing one decides.
-template <int LK>
+template <int LK, bool SH>
 __device__ __forceinline__ int label_of(const void* __restrict__ list, const float4* __restrict__ rec,
                                         const int* __restrict__ sid, const int* __restrict__ rec_sid, int start,
                                         int count, int nstructures, float x, float y, float z, int S, int& oob) {
@@ -174,7 +179,7 @@ __device__ __forceinline__ int label_of(const void* __restrict__ list, const flo
     } else {
       int key;
       float4 c;
-      entry<LK>(list, rec, sid, start + i, false, S, oob, key, c);
+      entry<LK, SH>(list, rec, sid, start + i, false, S, oob, key, c);
       if (inside_test(x - c.x, y - c.y, z - c.z, c.w) < 0) return __ldg(rec_sid + key);
     }
   }
@@ -236,7 +241,7 @@ __device__ __forceinline__ void jump_of(const JobDev& J, uint32_t wid, int s, in
 // compensation and the step's jump; the origin (spins0) and the flag word stay
 // in memory and are updated in place on the rare wrap / iteration-cap events
 // (except with moments, which read the origin every step).
-template <int MODE, int LK>
+template <int MODE, int LK, bool SH>
 __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1, double* s_mom) {
   constexpr bool kMom = (MODE & NZ_MODE_MOMENTS) != 0;
   constexpr bool kDisp = (MODE & kModeDisp) != 0;
@@ -307,9 +312,9 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     if (has_near && !near) cell_list(J, false, cell, start, count, oob);
     ScanOut r;
     constexpr bool kT64 = (MODE & NZ_MODE_TANGENT64) != 0;
-    if (!scan_cell<LK, kT64>(list, sph4, sidv, start, count, J.nstructures, lo, hi, x, y, z, label, a, jx, jy, jz,
+    if (!scan_cell<LK, kT64, SH>(list, sph4, sidv, start, count, J.nstructures, lo, hi, x, y, z, label, a, jx, jy, jz,
                              reach, J.S, oob, r)) {
-      label = label_of<LK>(list, sph4, sidv, J.rec_sid, start, count, J.nstructures, x, y, z, J.S, oob);
+      label = label_of<LK, SH>(list, sph4, sidv, J.rec_sid, start, count, J.nstructures, x, y, z, J.S, oob);
       if (kCheckBounds && (label < 0 || label > J.nstructures)) {
         oob = 1;
         label = J.nstructures;
@@ -325,7 +330,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
       // the full list: the near one was chosen for the old reach
       int fs, fc;
       cell_list(J, false, cell, fs, fc, oob);
-      scan_cell<LK, kT64>(LK ? J.idx : nullptr, LK ? J.rec4 : J.sph4, LK ? nullptr : J.sid, fs, fc, J.nstructures, lo,
+      scan_cell<LK, kT64, SH>(LK ? J.idx : nullptr, LK ? J.rec4 : J.sph4, LK ? nullptr : J.sid, fs, fc, J.nstructures, lo,
                           hi, x, y, z, label, a, jx, jy, jz, reach, J.S, oob, r);
     }
     jc = ref_min(jc, r.any_in ? r.fin : kBig);
@@ -435,14 +440,21 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
 
 // One work item: walkers [first, first + count) of job J, steps [step0, step1)
 // clamped to the job's protocol.
-template <int MODE, int LK>
-__device__ __forceinline__ void run_item(const JobDev& J, int first, int count, int step0, int step1, double* s_mom) {
+template <int MODE, int LK, bool SH>
+__device__ __forceinline__ void run_item(const JobDev& J, int first, int count, int step0, int step1, double* s_mom,
+                                         int flags = 0) {
   const int s0 = step0 + J.step_offset, s1 = min(step1 + J.step_offset, J.nsteps);
   if (MODE & NZ_MODE_MOMENTS) {
     for (int i = threadIdx.x; i < kMomentSteps * 6; i += blockDim.x) s_mom[i] = 0.0;
     __syncthreads();
   }
-  if (threadIdx.x < count && s0 < s1) walk_one<MODE, LK>(J, first + threadIdx.x, s0, s1, s_mom);
+  if (threadIdx.x < count && s0 < s1) {
+    walk_one<MODE, LK, SH>(J, first + threadIdx.x, s0, s1, s_mom);
+    if (flags) {
+      float4* c = J.comp + first + threadIdx.x;
+      c->w = __int_as_float(__float_as_int(c->w) | flags);
+    }
+  }
   if (MODE & NZ_MODE_MOMENTS) {
     __syncthreads();
     if (J.moments)
@@ -452,22 +464,81 @@ __device__ __forceinline__ void run_item(const JobDev& J, int first, int count, 
   }
 }
 
+// Staging a job's records into shared memory: one bulk copy (the TMA unit's
+// cp.async.bulk, global -> shared) completing on an mbarrier.  Sizes are
+// multiples of 16 bytes and both addresses 16-byte aligned (the host checks
+// the records' address; s_stage is 16-byte aligned).  Every wait is bounded.
+constexpr int kStageSpin = 1 << 20;  // try_wait polls before a copy is given up on
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  for (int i = 0; i < kStageSpin; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// Thread 0 only.  The CTA's generic-proxy reads of the previous contents of
+// s_stage ended at a barrier before this call; the proxy fence orders them
+// before the bulk copy's writes.
+__device__ __forceinline__ void stage_records(uint32_t bar, const float4* src, uint32_t bytes) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(s_stage)),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
 // Work items are CTAs' worth of walkers of one job.  SINGLE: one job passed by
 // value, item i = walkers [i*T, i*T + T).  Otherwise jobs and items come from
 // device arrays; with queue != null the grid is persistent and each CTA takes
 // items from *queue until none is left.
+// STAGE (batched, index lists): a job whose S records fit in stage_cap
+// records is walked with its records in shared memory (s_stage, stage_cap *
+// 16 bytes of dynamic shared memory); the copy is made when a CTA's item
+// belongs to a job other than the one already staged.  Larger jobs read
+// their records from global memory as without STAGE.  The records are the
+// same bytes either way, so the walk's results are identical.
 #ifdef NZ_FUSED_MAXNREG
 #define NZ_FUSED_BOUNDS __maxnreg__(NZ_FUSED_MAXNREG)
 #else
 #define NZ_FUSED_BOUNDS __launch_bounds__(kFusedMaxThreads, kFusedMinBlocks)
 #endif
-template <int MODE, int LK, bool SINGLE>
+template <int MODE, int LK, bool SINGLE, bool STAGE>
 __global__ void NZ_FUSED_BOUNDS
     walk_fused_kernel(const __grid_constant__ JobDev single, const nz_job* __restrict__ jobs,
-                      const nz_item* __restrict__ items, int n_items, int step0, int step1, int* queue) {
+                      const nz_item* __restrict__ items, int n_items, int step0, int step1, int* queue,
+                      int stage_cap) {
+  static_assert(!STAGE || (!SINGLE && LK != 0), "staging is for batched index-list walks");
   __shared__ int s_item;
   __shared__ double s_mom[(MODE & NZ_MODE_MOMENTS) ? kMomentSteps * 6 : 1];
   __shared__ JobDev s_job;
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ const float4* s_staged;  // the records now in s_stage (thread 0's bookkeeping)
+  __shared__ int s_use, s_broken, s_pending;
+  uint32_t phase = 0;  // parity of the barrier phase the next copy completes
+  if (STAGE) {
+    if (threadIdx.x == 0) {
+      mbar_init(smem_addr(&s_bar));
+      s_staged = nullptr;
+      s_broken = s_pending = 0;
+    }
+    __syncthreads();
+  }
   int it = blockIdx.x;
   for (;;) {
     if (queue) {
@@ -476,11 +547,16 @@ __global__ void NZ_FUSED_BOUNDS
       it = s_item;
       __syncthreads();
     }
-    if (it >= n_items) return;
+    if (it >= n_items) {
+      // a copy given up on may still be writing s_stage: wait for it (bounded)
+      // before the CTA's shared memory is released
+      if (STAGE && threadIdx.x == 0 && s_pending) mbar_wait_bounded(smem_addr(&s_bar), phase);
+      return;
+    }
     if (SINGLE) {
       const int first = it * int(blockDim.x);
       const int count = min(int(blockDim.x), single.nwalkers - first);
-      run_item<MODE, LK>(single, first, count, step0, step1, s_mom);
+      run_item<MODE, LK, false>(single, first, count, step0, step1, s_mom);
     } else {
       // every thread of the CTA works on the same job: its descriptor lives
       // in shared memory, not in each thread's registers
@@ -489,12 +565,56 @@ __global__ void NZ_FUSED_BOUNDS
         const nz_job& a = jobs[wi.job];
         s_job = make_job(a.sub, a.G, a.Garea, a.nsteps, a.dt, a.draws, a.mode, a.state, a.moments);
         s_job.step_offset = a.step_offset;
+        if (STAGE) {
+          const float4* src = s_job.rec4;
+          const int S = s_job.S;
+          int use = 0;
+          if (!s_broken && S > 0 && S <= stage_cap && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+            if (src == s_staged) {
+              use = 1;
+            } else {
+              stage_records(smem_addr(&s_bar), src, uint32_t(S) * 16u);
+              s_pending = 1;
+              use = 2;
+            }
+          }
+          s_use = use;
+        }
       }
       __syncthreads();
-      run_item<MODE, LK>(s_job, wi.first, wi.count, step0, step1, s_mom);
+      if (STAGE) {
+        int use = s_use;
+        int flags = 0;
+        if (use == 2) {
+          // every thread observes the copy's completion on the barrier
+          const bool done = mbar_wait_bounded(smem_addr(&s_bar), phase);
+          const int late = __syncthreads_or(!done);
+          if (late) {  // walk from global memory; stage nothing more
+            use = 0;
+            flags = kFlagStageTimeout;
+            if (threadIdx.x == 0) {
+              s_broken = 1;
+              s_staged = nullptr;
+            }
+          } else {
+            phase ^= 1u;
+            if (threadIdx.x == 0) {
+              s_staged = s_job.rec4;
+              s_pending = 0;
+            }
+          }
+        }
+        if (use) run_item<MODE, LK, true>(s_job, wi.first, wi.count, step0, step1, s_mom);
+        else run_item<MODE, LK, false>(s_job, wi.first, wi.count, step0, step1, s_mom, flags);
+      } else {
+        run_item<MODE, LK, false>(s_job, wi.first, wi.count, step0, step1, s_mom);
+      }
       __syncthreads();
     }
-    if (!queue) return;
+    if (!queue) {
+      if (STAGE && threadIdx.x == 0 && s_pending) mbar_wait_bounded(smem_addr(&s_bar), phase);
+      return;
+    }
   }
 }
 
@@ -594,9 +714,32 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
   return j;
 }
 
+// Dynamic shared memory of the staged kernel for stage_cap records, after
+// setting its attributes: the largest allowed size (once per device) and a
+// carveout that leaves room for the CTAs the register budget allows at this
+// CTA size, the rest staying L1.
+template <int MODE, int LK>
+size_t stage_setup(int stage_cap, int threads) {
+  const size_t bytes = size_t(stage_cap) * 16;
+  if (LK == 0 || stage_cap <= 0) return 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) {
+    static std::once_flag once[kMaxDevices];
+    std::call_once(once[dev], [] {
+      cudaFuncSetAttribute(walk_fused_kernel<MODE, LK, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kMaxStageRecords * 16);
+    });
+  }
+  const int ctas = std::max(1, kFusedMinBlocks * kFusedMaxThreads / threads);
+  const size_t need = size_t(ctas) * (bytes + 2048);
+  const int pct = int(std::min<size_t>(100, (100 * need + kSmemPerSm - 1) / kSmemPerSm));
+  cudaFuncSetAttribute(walk_fused_kernel<MODE, LK, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  return bytes;
+}
+
 template <int MODE, int LK>
 void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0, int step1,
-                 int* queue, int grid, int threads, cudaStream_t st) {
+                 int* queue, int grid, int threads, int stage_cap, cudaStream_t st) {
   // the kernel keeps little in shared memory: prefer the whole carveout for
   // L1.  Function attributes belong to a device's context, so this is done
   // once per device (and once across threads).
@@ -604,20 +747,33 @@ void launch_mode(const JobDev& single, const nz_job* jobs, const nz_item* items,
   if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) {
     static std::once_flag once[kMaxDevices];
     std::call_once(once[dev], [] {
-      cudaFuncSetAttribute(walk_fused_kernel<MODE, LK, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-      cudaFuncSetAttribute(walk_fused_kernel<MODE, LK, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+      cudaFuncSetAttribute(walk_fused_kernel<MODE, LK, false, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           0);
+      cudaFuncSetAttribute(walk_fused_kernel<MODE, LK, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           0);
     });
   }
+  if constexpr (LK != 0) {
+    if (jobs && stage_cap > 0) {
+      const size_t smem = stage_setup<MODE, LK>(stage_cap, threads);
+      walk_fused_kernel<MODE, LK, false, true>
+          <<<grid, threads, smem, st>>>(single, jobs, items, n_items, step0, step1, queue, stage_cap);
+      return;
+    }
+  }
   if (jobs)
-    walk_fused_kernel<MODE, LK, false><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
+    walk_fused_kernel<MODE, LK, false, false>
+        <<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue, 0);
   else
-    walk_fused_kernel<MODE, LK, true><<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue);
+    walk_fused_kernel<MODE, LK, true, false>
+        <<<grid, threads, 0, st>>>(single, jobs, items, n_items, step0, step1, queue, 0);
 }
 
 template <int LK>
 int launch_lk(int mode, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items, int step0,
-              int step1, int* queue, int grid, int threads, cudaStream_t st) {
-#define NZ_LAUNCH(M) launch_mode<(M), LK>(single, jobs, items, n_items, step0, step1, queue, grid, threads, st)
+              int step1, int* queue, int grid, int threads, int stage_cap, cudaStream_t st) {
+#define NZ_LAUNCH(M) \
+  launch_mode<(M), LK>(single, jobs, items, n_items, step0, step1, queue, grid, threads, stage_cap, st)
   switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS | NZ_MODE_TANGENT64 | kModeDisp)) {
     case NZ_MODE_PHI | NZ_MODE_TANGENT64: NZ_LAUNCH(NZ_MODE_PHI | NZ_MODE_TANGENT64); break;
     case NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_TANGENT64: NZ_LAUNCH(NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_TANGENT64); break;
@@ -636,41 +792,52 @@ int launch_lk(int mode, const JobDev& single, const nz_job* jobs, const nz_item*
 }
 
 // jobs == null: the single job `single` with n_items CTAs of kFusedThreads walkers.
+// stage_cap > 0 (batched index-list walks): stage the records of jobs of at
+// most stage_cap records in shared memory.
 int launch_fused(int mode, int lk, const JobDev& single, const nz_job* jobs, const nz_item* items, int n_items,
-                 int step0, int step1, int* queue, int grid, int threads, cudaStream_t st) {
+                 int step0, int step1, int* queue, int grid, int threads, cudaStream_t st, int stage_cap) {
   switch (lk) {
-    case 0: return launch_lk<0>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
-    case 2: return launch_lk<2>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
-    case 4: return launch_lk<4>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, st);
+    case 0: return launch_lk<0>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, 0, st);
+    case 2:
+      return launch_lk<2>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, stage_cap, st);
+    case 4:
+      return launch_lk<4>(mode, single, jobs, items, n_items, step0, step1, queue, grid, threads, stage_cap, st);
     default: return set_error(NZ_ERR_ARG, "fused walk: list kind %d is not 0, 2 or 4", lk);
   }
 }
 
+template <int MODE, int LK>
+cudaError_t occupancy_mode(int threads, int stage_cap, int* blocks_per_sm) {
+  if constexpr (LK != 0) {
+    if (stage_cap > 0) {
+      const size_t smem = stage_setup<MODE, LK>(stage_cap, threads);
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<MODE, LK, false, true>,
+                                                           threads, smem);
+    }
+  }
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<MODE, LK, false, false>,
+                                                       threads, 0);
+}
+
 template <int LK>
-cudaError_t occupancy_lk(int mode, int threads, int* blocks_per_sm) {
+cudaError_t occupancy_lk(int mode, int threads, int stage_cap, int* blocks_per_sm) {
   switch (mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS)) {
-    case NZ_MODE_PHI:
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<NZ_MODE_PHI, LK, false>,
-                                                           threads, 0);
-    case NZ_MODE_SIG:
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, walk_fused_kernel<NZ_MODE_SIG, LK, false>,
-                                                           threads, 0);
-    case NZ_MODE_PHI | NZ_MODE_SIG:
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          blocks_per_sm, walk_fused_kernel<NZ_MODE_PHI | NZ_MODE_SIG, LK, false>, threads, 0);
+    case NZ_MODE_PHI: return occupancy_mode<NZ_MODE_PHI, LK>(threads, stage_cap, blocks_per_sm);
+    case NZ_MODE_SIG: return occupancy_mode<NZ_MODE_SIG, LK>(threads, stage_cap, blocks_per_sm);
+    case NZ_MODE_PHI | NZ_MODE_SIG: return occupancy_mode<NZ_MODE_PHI | NZ_MODE_SIG, LK>(threads, stage_cap, blocks_per_sm);
     default: return cudaErrorInvalidValue;
   }
 }
 
-int occupancy_fused(int mode, int lk, int threads, int* blocks_per_sm) {
+int occupancy_fused(int mode, int lk, int threads, int* blocks_per_sm, int stage_cap) {
   const int m = mode & (NZ_MODE_PHI | NZ_MODE_SIG | NZ_MODE_MOMENTS);
   if (m != NZ_MODE_PHI && m != NZ_MODE_SIG && m != (NZ_MODE_PHI | NZ_MODE_SIG))
     return set_error(NZ_ERR_ARG, "occupancy: unsupported batch mode %d", mode);
   cudaError_t e;
   switch (lk) {
-    case 0: e = occupancy_lk<0>(mode, threads, blocks_per_sm); break;
-    case 2: e = occupancy_lk<2>(mode, threads, blocks_per_sm); break;
-    case 4: e = occupancy_lk<4>(mode, threads, blocks_per_sm); break;
+    case 0: e = occupancy_lk<0>(mode, threads, 0, blocks_per_sm); break;
+    case 2: e = occupancy_lk<2>(mode, threads, stage_cap, blocks_per_sm); break;
+    case 4: e = occupancy_lk<4>(mode, threads, stage_cap, blocks_per_sm); break;
     default: return set_error(NZ_ERR_ARG, "occupancy: list kind %d is not 0, 2 or 4", lk);
   }
   if (e != cudaSuccess) return set_error(NZ_ERR_CUDA, "occupancy: %s", cudaGetErrorString(e));

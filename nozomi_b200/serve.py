@@ -50,7 +50,7 @@ import torch
 
 from . import engine
 from . import _lib as L
-from .batch import LIST_BITS, JobSpec, SubstrateCache, _job_table, _items, _sort_table, batch_grid, list_groups
+from .batch import JobSpec, SubstrateCache, _items, _job_table, _sort_table, batch_grid, launch_batch, list_groups
 from .simulate import Tuning
 from .substrates import cell_grid
 from .waveforms import step_tables
@@ -114,7 +114,7 @@ class Server:
         self.dev = dev
         self.compute = torch.cuda.current_stream(dev)
         self.side = torch.cuda.Stream(dev)
-        self.grids = {lk: batch_grid(threads, lk) for lk in (0, 2, 4)}
+        self.grids = {lk: batch_grid(threads, lk, self.tuning.stage) for lk in (0, 2, 4)}
         self.queue = torch.zeros(3, dtype=torch.int32, device=dev)
         self.sort_scratch = torch.empty(1, dtype=torch.uint8, device=dev)
         self.clock = time.perf_counter
@@ -254,11 +254,8 @@ class Server:
                                       stream), "nz_batch_sort")
             self.queue.zero_()
             for g, (lk, items) in enumerate(groups):
-                L.check(lib.nz_walk_batch(ctypes.c_void_p(table.data_ptr()), len(jobs),
-                                          ctypes.c_void_p(items.data_ptr()), int(items.shape[0]),
-                                          L.MODE_PHI | LIST_BITS[lk], 0, k,
-                                          ctypes.c_void_p(self.queue.data_ptr() + 4 * g), self.grids[lk],
-                                          self.threads, stream), "nz_walk_batch")
+                launch_batch(table, len(jobs), items, lk, 0, k, self.queue.data_ptr() + 4 * g, self.grids[lk],
+                             self.threads, self.tuning.stage, stream)
             e1.record(self.compute)
             finished, ws = [], 0
             for t in self.active:

@@ -31,6 +31,7 @@ class Tuning:
     near_margin: float | None = 0.5  # margin of the near lists (None: full lists only)
     lists: str = "index"          # the fused walk's list form: "index" (16/32-bit) or "records"
     near_shape: str = "round"     # near lists by the Euclidean sphere-to-cell test ("round") or the box test
+    stage: int = 0                # batched walk: records a CTA stages in shared memory (0: none)
 
 
 def idx_bytes_for(lists: str):

@@ -250,6 +250,16 @@ def test_invalid_arguments_rejected_without_gpu():
     refused(lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_PHI, 0, 100, FAKE, 148, 512, None), "nz_walk_batch")
     refused(lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_PHI, 0, 100, None, 148, 128, None), "nz_walk_batch")
     refused(lib.nz_walk_batch(FAKE, 3, FAKE, 10, _lib.MODE_MOMENTS, 0, 100, FAKE, 148, 128, None), "nz_walk_batch")
+    # staged batched walk: record lists, capacity out of range, the same shape checks
+    staged = "nz_walk_batch_staged"
+    idx = _lib.MODE_PHI | _lib.LIST_IDX16
+    refused(lib.nz_walk_batch_staged(FAKE, 3, FAKE, 10, _lib.MODE_PHI, 0, 100, FAKE, 148, 128, 1024, None), staged)
+    refused(lib.nz_walk_batch_staged(FAKE, 3, FAKE, 10, idx, 0, 100, FAKE, 148, 128, -1, None), staged)
+    refused(lib.nz_walk_batch_staged(FAKE, 3, FAKE, 10, idx, 0, 100, FAKE, 148, 128, _lib.MAX_STAGE_RECORDS + 1,
+                                     None), staged)
+    refused(lib.nz_walk_batch_staged(FAKE, 3, FAKE, 10, idx, 0, 100, FAKE, 148, 48, 1024, None), staged)
+    refused(lib.nz_walk_batch_staged(FAKE, 3, FAKE, 10, idx, 0, 100, None, 148, 128, 1024, None), staged)
+    assert lib.nz_walk_batch_staged(FAKE, 3, FAKE, 0, idx, 0, 100, FAKE, 148, 128, 1024, None) == 0
     # plain step: unknown mode bits, phase without directions, null positions
     wk = _lib.Walkers()
     wk.N, wk.spins, wk.spins0 = N, FAKE, FAKE

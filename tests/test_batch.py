@@ -113,3 +113,47 @@ def test_autotune_small(tmp_path):
     assert len(rep["trials"]) >= 3
     t2, threads2, rep2 = autotune(specs, space=space, cache_file=cache_file)
     assert rep2["cached"] and threads2 == threads and t2 == t
+
+
+@pytest.mark.parametrize("threads", [128, 256])
+def test_staged_records_equal_global_records(batch_result, threads):
+    """nz_walk_batch_staged (each job's records copied into the CTA's shared
+    memory when they fit) against the same batch reading its records from
+    global memory: signals and every walker's state bit for bit, with the
+    capacity between the jobs' record counts so that some jobs are staged
+    and some are not; no copy timed out."""
+    import dataclasses
+    from nozomi_b200 import _lib as L
+    from nozomi_b200.batch import BatchRun
+    specs, cache, tuning, run, sig = batch_result
+    S = sorted(cache.get(sp.key, sp.substrate, sp.D, sp.T2, tuning).S for sp in specs)
+    assert S[0] < S[-1]
+    staged = dataclasses.replace(tuning, stage=S[len(S) // 2])
+    ref = BatchRun(specs, tuning=tuning, threads=threads, cache=cache).step()
+    got = BatchRun(specs, tuning=staged, threads=threads, cache=cache).step()
+    for i in range(len(specs)):
+        # the signal sums to FP64 summation order (walkers of one re-binning
+        # bin may be stored in any order); every walker's state, by walker id,
+        # bit for bit
+        np.testing.assert_allclose(got.signals()[i], ref.signals()[i], rtol=0, atol=1e-12)
+        a, b = got.final_state(i), ref.final_state(i)
+        ia = torch.argsort(a.org[:, 3].view(torch.int32))
+        ib = torch.argsort(b.org[:, 3].view(torch.int32))
+        for name in ("pos", "org", "phi", "comp"):
+            x, y = getattr(a, name)[ia].view(torch.int32), getattr(b, name)[ib].view(torch.int32)
+            assert torch.equal(x, y), (i, name)
+        flags = a.comp[:, 3].view(torch.int32)
+        assert not bool(((flags & L.FLAG_STAGE_TIMEOUT) != 0).any())
+
+
+def test_staged_batch_refusals():
+    """Staging is for index lists and at most MAX_STAGE_RECORDS records."""
+    import ctypes
+    from nozomi_b200 import _lib as L
+    lib = L.load()
+    occ = ctypes.c_int(0)
+    assert lib.nz_batch_occupancy_staged(L.MODE_PHI | L.LIST_IDX16, 128, 4096, ctypes.byref(occ)) == 0
+    assert occ.value >= 1
+    assert lib.nz_batch_occupancy_staged(L.MODE_PHI, 128, 4096, ctypes.byref(occ)) != 0  # record lists
+    assert lib.nz_batch_occupancy_staged(L.MODE_PHI | L.LIST_IDX16, 128, L.MAX_STAGE_RECORDS + 1,
+                                         ctypes.byref(occ)) != 0

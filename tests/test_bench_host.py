@@ -84,7 +84,8 @@ def test_reference_arm_prints_the_contract_line():
     from oracle.build import reference_named
     if reference_named("batched_job0_cpu_8k") is None or reference_named("packed_cpu_16k") is None:
         pytest.skip("oracle/_ref reference build absent (the reference tree was absent at build)")
-    for extra, wl in (((), bench.BATCH_WORKLOAD.format(jobs=64, scale=1.0)), (("--workload", "packed"), bench.WORKLOAD)):
+    for extra, wl in (((), bench.BATCH_WORKLOAD.format(jobs=64, scale=1.0, a0=10, a1=500)),
+                      (("--workload", "packed"), bench.WORKLOAD)):
         d = _reference_line(*extra)
         for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
                   "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
