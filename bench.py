@@ -110,6 +110,9 @@ def parse(argv=None):
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="torch.distributed backend for --gpus N > 1 (gloo: host-side collectives, for checking the "
+                         "multi-rank path where NCCL is not usable)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference_gpu"],
                     help="reference: the reference's walk on the host cores; reference_gpu: the reference's own "
                          "CUDA kernel (baseline/_ref build) on this GPU, one launch per waveform sample")
@@ -523,7 +526,7 @@ def run_packed(args):
         # collective with an error instead of a hang (set-up before the first
         # barrier takes well under this)
         from nozomi_b200.shard import init_process_group
-        init_process_group("nccl", timeout_s=180)
+        init_process_group(args.dist_backend, timeout_s=180)
     engine.require_cuda()
     sub, pg, dirs, bvals = workload_packed()
     # launch shape tuned for this workload by sweeps on a B200: 0.5 um cells,
@@ -806,7 +809,7 @@ def run_batched(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if world > 1:
-        init_process_group("nccl", timeout_s=180)
+        init_process_group(args.dist_backend, timeout_s=180)
     engine.require_cuda()
     t0 = time.perf_counter()
     all_specs = mixed_specs(seed=4, n_jobs=args.jobs, walker_scale=args.walker_scale, axons=tuple(args.axons))
@@ -923,13 +926,26 @@ def run_batched(args):
                 "item and re-binning tables built and uploaded, walkers packed, every chunk re-binned and walked "
                 "(eager launches), signals reduced and copied back; cell lists from a warm substrate cache",
         "max_signal_diff_vs_graph": e2e_diff}
+    launch_ms = walk_ms / max(len(ev), 1)
+    ws_launch = sum(chunk_ws) / max(len(chunk_ws), 1)
+    state_bytes = 128 * sum(c["sort_walkers"] for c in run.chunks) / max(len(run.chunks), 1)
+    shape = {"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": threads,
+             "lists": tuning.lists, "near_shape": tuning.near_shape}
     if world > 1:
         if rank == 0:
+            # the issue roofline of rank 0's own batched launches (the host-core
+            # baseline and its work counts are measured at N=1 only)
+            roof_issue = rooflines("batched", kernel_ws_s, ws_launch, launch_ms, state_bytes, clk, sms,
+                                   fp32_peak_tflops, None, None, shape=shape)[0]
             print(json.dumps({"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
                               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                               "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
                               "data": "synthetic (seeded substrates, protocols and walkers)", "config": config,
-                              "e2e": e2e, "gpu_launches": run.launches() * args.steps, "clocks": clk}), flush=True)
+                              "e2e": e2e, "gpu_launches": run.launches() * args.steps,
+                              "kernel": {"name": "walk_fused_kernel (batched form, nz_walk_batch), rank 0",
+                                         "launches": len(ev), "avg_launch_ms": launch_ms,
+                                         "kernel_walker_steps_per_s": kernel_ws_s},
+                              "roofline": roof_issue, "cpu_baseline": None, "clocks": clk}), flush=True)
         dist.barrier()
         dist.destroy_process_group()
         return 0
@@ -972,13 +988,9 @@ def run_batched(args):
         wk_all = {k: float(np.mean([w[k] for w in works])) for k in works[0]}
     ndir_mean = sum(sp.walker_steps * np.asarray(sp.dirs).shape[1] for sp in specs) / ws
     F_alg = None if wk_all is None else 10 * wk_all["spheres_in_reach"] + 36 * wk_all["solves_in_reach"] + 6 * ndir_mean
-    launch_ms = walk_ms / max(len(ev), 1)
-    ws_launch = sum(chunk_ws) / max(len(chunk_ws), 1)
-    state_bytes = 128 * sum(c["sort_walkers"] for c in run.chunks) / max(len(run.chunks), 1)
     roof_issue, roof_fp32, roof_hbm = rooflines(
         "batched", kernel_ws_s, ws_launch, launch_ms, state_bytes, clk, sms, fp32_peak_tflops, F_alg, wk_all,
-        shape={"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": threads,
-               "lists": tuning.lists, "near_shape": tuning.near_shape})
+        shape=shape)
     line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32",
