@@ -80,21 +80,21 @@ KERNEL_SOURCES = ("nozomi_b200/csrc/walk_fused.cu", "nozomi_b200/csrc/nz_common.
 # dram__bytes_write.sum) of the captured launch, divided by the walker-steps
 # that launch ran; kernel_sha: the sources' hash at capture.
 PROFILED = {
-    "packed": {"kernel_sha": "42d7c0b4116230f5", "warp_inst_per_walker_step": 58.857,
-               "dram_bytes_per_walker_step": 0.9932,
+    "packed": {"kernel_sha": "f9ddf04e9e187c30", "warp_inst_per_walker_step": 56.421,
+               "dram_bytes_per_walker_step": 0.9975,
                "shape": {"cell": 0.5, "near_margin": 0.5, "coarsen": 8, "threads": 128, "lists": "index",
                          "near_shape": "round"},
                "capture": "walk_fused_kernel<PHI, idx16> launch 3 of `python bench.py --workload packed --walkers "
                           "1000000 --steps-per-launch 200 --steps 1 --warmup 1 --no-cpu-baseline --e2e-steps 0` "
-                          "(200,000,000 walker-steps): 11,771,485,495 warp instructions, 198.6 MB DRAM"},
-    "batched": {"kernel_sha": "42d7c0b4116230f5", "warp_inst_per_walker_step": 43.418,
-                "dram_bytes_per_walker_step": 0.2360,
+                          "(200,000,000 walker-steps): 11,284,186,998 warp instructions, 199.5 MB DRAM"},
+    "batched": {"kernel_sha": "f9ddf04e9e187c30", "warp_inst_per_walker_step": 41.074,
+                "dram_bytes_per_walker_step": 0.2405,
                 "shape": {"cell": 1.0, "near_margin": 0.5, "coarsen": 4, "threads": 256, "lists": "index",
                           "near_shape": "round"},
                 "capture": "walk_fused_kernel<PHI, idx16> launch 2 of `python bench.py --walker-scale 0.1 --steps 1 "
                            "--warmup 1 --no-serving --no-plain --no-cpu-baseline --e2e-steps 0 --no-autotune --cell 1.0 "
                            "--coarsen 4 --steps-per-launch 2000 --threads 256` (64 jobs, 2,407,477,000 walker-steps): "
-                           "104,528,520,791 warp instructions, 568.2 MB DRAM"},
+                           "98,884,211,945 warp instructions, 579.1 MB DRAM"},
 }
 
 

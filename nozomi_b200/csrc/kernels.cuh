@@ -71,6 +71,7 @@ constexpr int kModeDisp = 32;
 
 struct JobDev {
   Grid g;
+  float idLx, idLy, idLz;  // 1 / cell edge (the fused walk's per-step cell)
   int nstructures;
   const float4* sph4;
   const int* sid;
@@ -94,6 +95,7 @@ struct JobDev {
   int step_offset;
   // near lists (null sph4, or null near_idx in index form: none)
   float near_margin;
+  float near_cut;  // (near_margin - tol - 2 nm) / 1.02: the near test's bound on distance + reach
   const int* near_start;
   const int* near_count;
   const float4* near_sph4;

@@ -196,15 +196,23 @@ __device__ __forceinline__ void label_bounds(const JobDev& J, int L, int& lo, in
   }
 }
 
-// Cell of the walker at the start of a step and the cell's low corner.
-__device__ __forceinline__ int step_cell(const Grid& g, float x, float y, float z, float& lox, float& loy,
+// Cell of the walker at the start of a step and the cell's low corner: the
+// clamped floor of (x + L/2) times the reciprocal cell edge.  For a walker
+// within a rounding error of a cell face this can be the neighbour of the
+// reference's division-based cell (cell_of); the walk's result is the same
+// with either: the near test measures the walker's distance to the cell taken
+// here, and the full lists reach jump_tol beyond their cell, so both lists
+// hold every sphere the iteration can touch or be inside.
+__device__ __forceinline__ int step_cell(const JobDev& J, float x, float y, float z, float& lox, float& loy,
                                          float& loz) {
-  float cx, cy, cz;
-  const int c = cell_of(g, x, y, z, cx, cy, cz);
+  const Grid& g = J.g;
+  const float cz = ref_min(g.nLz - 1, ref_max(0, floorf((z + g.Lz / 2) * J.idLz)));
+  const float cy = ref_min(g.nLy - 1, ref_max(0, floorf((y + g.Ly / 2) * J.idLy)));
+  const float cx = ref_min(g.nLx - 1, ref_max(0, floorf((x + g.Lx / 2) * J.idLx)));
   lox = cx * g.dLx - g.Lx / 2;
   loy = cy * g.dLy - g.Ly / 2;
   loz = cz * g.dLz - g.Lz / 2;
-  return c;
+  return int(cz * g.nLx * g.nLy + cy * g.nLx + cx);
 }
 
 // Start and count of cell `cell`'s list (the near list when near).  In the
@@ -226,6 +234,12 @@ __device__ __forceinline__ void cell_list(const JobDev& J, bool near, int cell, 
     }
   }
 }
+
+// This iteration's reach |j| * jump_remaining, from the hardware reciprocal
+// square root: within a few ulp of sqrtf, far inside the 2 % + 2 nm of slack
+// of the only two uses (the near test and the first-pass filter), which
+// decide what is scanned, never a result.
+__device__ __forceinline__ float reach_of(float a, float jr) { return a * rsqrtf(fmaxf(a, 1e-30f)) * jr; }
 
 // Draw `draw` of step s scaled by ds.
 __device__ __forceinline__ void jump_of(const JobDev& J, uint32_t wid, int s, int draw, float ds, float& jx, float& jy,
@@ -284,7 +298,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
   float ds = sqrtf(2 * __ldg(J.D + label) * dt);
   int oob = 0;  // bounds-checked build: an index was out of range
   if (s < s1) {
-    cell = step_cell(J.g, x, y, z, lox, loy, loz);
+    cell = step_cell(J, x, y, z, lox, loy, loz);
     cell_list(J, has_near, cell, pstart, pcount, oob);
     jump_of(J, wid, s, 0, ds, jx, jy, jz);
     draw = 1;
@@ -293,17 +307,19 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
     niter++;
     float jc = jr;
     float a = jx * jx + jy * jy + jz * jz;
-    float reach = sqrtf(a) * jr;
+    float reach = reach_of(a, jr);
     // Near list when everything this iteration can touch lies within its
     // margin of the step's cell: distance from the walker to the cell plus
-    // the reach, with 2 % + 2 nm of slack against rounding.
+    // the reach, with 2 % + 2 nm of slack against rounding
+    // ((dist + reach) * 1.02 + tol + 2 nm <= margin, as dist^2 <= t^2 with
+    // t = near_cut - reach).
     bool near = false;
     if (has_near) {
       const float ex = fmaxf(0.f, fmaxf(lox - x, x - (lox + J.g.dLx)));
       const float ey = fmaxf(0.f, fmaxf(loy - y, y - (loy + J.g.dLy)));
       const float ez = fmaxf(0.f, fmaxf(loz - z, z - (loz + J.g.dLz)));
-      const float dist = sqrtf(ex * ex + ey * ey + ez * ez);
-      near = (dist + reach) * 1.02f + kTol + 2e-3f <= J.near_margin;
+      const float t = J.near_cut - reach;
+      near = t >= 0.f && ex * ex + ey * ey + ez * ez <= t * t;
     }
     const void* list = LK ? (near ? J.near_idx : J.idx) : nullptr;
     const float4* sph4 = LK ? J.rec4 : (near ? J.near_sph4 : J.sph4);
@@ -325,7 +341,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
         ds_label = label;
         jump_of(J, wid, s, 0, ds, jx, jy, jz);
         a = jx * jx + jy * jy + jz * jz;
-        reach = sqrtf(a) * jr;
+        reach = reach_of(a, jr);
       }
       // the full list: the near one was chosen for the old reach
       int fs, fc;
@@ -420,7 +436,7 @@ __device__ __forceinline__ void walk_one(const JobDev& J, int w, int s0, int s1,
         ds = sqrtf(2 * __ldg(J.D + label) * dt);
         ds_label = label;
       }
-      cell = step_cell(J.g, x, y, z, lox, loy, loz);
+      cell = step_cell(J, x, y, z, lox, loy, loz);
       cell_list(J, has_near, cell, pstart, pcount, oob);
     }
     if (s < s1) jump_of(J, wid, next_step, next_draw, ds, jx, jy, jz);
@@ -676,12 +692,16 @@ __host__ __device__ JobDev make_job(const nz_substrate& sub, const float* G, con
   j.step_offset = 0;
   j.g = Grid{sub.grid.Lx, sub.grid.Ly, sub.grid.Lz, sub.grid.dLx, sub.grid.dLy, sub.grid.dLz,
              float(sub.grid.nx), float(sub.grid.ny), float(sub.grid.nz)};
+  j.idLx = 1.0f / sub.grid.dLx;
+  j.idLy = 1.0f / sub.grid.dLy;
+  j.idLz = 1.0f / sub.grid.dLz;
   j.nstructures = sub.nstructures;
   j.sph4 = reinterpret_cast<const float4*>(sub.cell_sph4);
   j.sid = sub.cell_sid;
   j.cell_start = sub.cell_start;
   j.cell_count = sub.cell_count;
   j.near_margin = sub.near_margin;
+  j.near_cut = (sub.near_margin - kTol - 2e-3f) / 1.02f;
   j.near_start = sub.near_start;
   j.near_count = sub.near_count;
   j.near_sph4 = reinterpret_cast<const float4*>(sub.near_sph4);
