@@ -12,7 +12,7 @@ Per job, three comparisons on the same seeded walkers and draws:
   accrual    the batched signal against the FP64 signal of the same FP32
              trajectories (the oracle sums every phase increment in FP64):
              the error of the FP32 Kahan phase and FP32 per-walker cos/sin,
-             bar 1e-3 (the north-star bar);
+             bar 1e-3 (the target signal error);
   walk       the batched signal against the full-FP64 oracle walk.  FP32 and
              FP64 collision decisions in the 1e-4 um tolerance shells round
              differently and decorrelate the walkers, so the two walks agree

@@ -138,7 +138,7 @@ def test_phase_accrual_packed_workload():
     substrate through all 6000 steps, 30 directions x 4 b.  The fused walk
     (Kahan Phi) against the exact FP64 phase of the same FP32 trajectories
     from the oracle: positions bit for bit, signal within 1e-5 (the Kahan
-    bar; the north-star bar is 1e-3)."""
+    bar; the target signal error is 1e-3)."""
     from nozomi_b200 import engine
     from nozomi_b200.simulate import DwiRun, Tuning, device_substrate
     from nozomi_b200.waveforms import step_tables
