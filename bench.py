@@ -148,6 +148,9 @@ def parse(argv=None):
     ap.add_argument("--serve-cell", type=float, default=None, help="serving: cell edge of the cached lists, um")
     ap.add_argument("--serve-coarsen", type=int, default=None, help="serving: re-binning bins in cells per axis")
     ap.add_argument("--max-requests", type=int, default=None, help="serving: requests per rate at most")
+    ap.add_argument("--serve-max-backlog", type=float, default=None,
+                    help="serving: shed a request on arrival when the backlog would take longer than this many "
+                         "seconds at the recent throughput (default: no shedding)")
     ap.add_argument("--jobs", type=int, default=64, help="batched: number of substrates")
     ap.add_argument("--walker-scale", type=float, default=1.0, help="batched: scale of the walker counts")
     ap.add_argument("--axons", type=lambda v: [int(a) for a in v.split(",")], default=[10, 500],
@@ -765,7 +768,7 @@ def plain_leg(specs, positions, sig_batched, every: int):
     return ws / (ms * 1e-3), len(sel), ws, err
 
 
-def serving_leg(pairs, tuning, threads, max_requests=None):
+def serving_leg(pairs, tuning, threads, max_requests=None, max_backlog_s=None):
     """Poisson request streams (configs of the mixed workload's distribution,
     substrates reused with probability 0.7) through the continuous-batching
     server, one stream per (rate, window).  Returns per-rate statistics,
@@ -782,7 +785,7 @@ def serving_leg(pairs, tuning, threads, max_requests=None):
         t0 = time.perf_counter()
         reqs = request_stream(rate, window, seed=5, max_requests=max_requests)
         gen_s += time.perf_counter() - t0
-        srv = Server(tuning=tuning, threads=threads, cache=cache)
+        srv = Server(tuning=tuning, threads=threads, cache=cache, max_backlog_s=max_backlog_s)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         done = srv.serve(reqs)
@@ -790,7 +793,8 @@ def serving_leg(pairs, tuning, threads, max_requests=None):
         st = latency_stats(done)
         st.update({"rate_req_s": rate, "arrival_window_s": window, "requests": len(reqs),
                    "walker_steps": srv.walker_steps, "walker_steps_per_s": srv.walker_steps / wall, "wall_s": wall,
-                   "rounds": srv.rounds, "failed": sum(t.error is not None for t in done)})
+                   "rounds": srv.rounds, "failed": sum(t.error is not None and not t.shed for t in done),
+                   "shed": sum(t.shed for t in done), "max_backlog_s": max_backlog_s})
         per_rate.append(st)
         done_all += done
     return per_rate, {"hits": cache.hits, "misses": cache.misses}, gen_s, done_all
@@ -962,7 +966,7 @@ def run_batched(args):
         pairs = [tuple(float(v) for v in p.split(":")) for p in args.serve.split(",") if p]
         stune = Tuning(cell=args.serve_cell or tuning.cell, coarsen=args.serve_coarsen or tuning.coarsen,
                        near_margin=tuning.near_margin, by_label=tuning.by_label)
-        per_rate, sc, sgen, _ = serving_leg(pairs, stune, threads, args.max_requests)
+        per_rate, sc, sgen, _ = serving_leg(pairs, stune, threads, args.max_requests, args.serve_max_backlog)
         serving = {"per_rate": per_rate, "substrate_cache": sc, "substrate_generation_s": sgen,
                    "cell_um": stune.cell, "rebin_coarsen": stune.coarsen,
                    "rounds": "time-bounded (about 50 ms at the measured throughput, 100-4000 steps)",
@@ -1037,7 +1041,7 @@ def run_serving(args):
     pairs = [tuple(float(v) for v in p.split(":")) for p in args.serve.split(",") if p]
     clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
-    per_rate, sc, sgen, all_done = serving_leg(pairs, tuning, args.threads, args.max_requests)
+    per_rate, sc, sgen, all_done = serving_leg(pairs, tuning, args.threads, args.max_requests, args.serve_max_backlog)
     clk = clocks.stop()
     sample = all_done[:: max(1, len(all_done) // 8)][:8]
     stream = torch.cuda.current_stream()
@@ -1063,7 +1067,8 @@ def run_serving(args):
             "config": {"workload": "serving: Poisson arrivals per rate, substrates of 10-500 beaded axons reused "
                                    "with probability 0.7, 1e4-5e5 walkers, 2000-8000 steps at 5 us, 6-60 directions, "
                                    "b<=3 ms/um^2, seed 5", "rates_and_windows": args.serve,
-                       "max_requests_per_rate": args.max_requests, "threads": args.threads,
+                       "max_requests_per_rate": args.max_requests, "max_backlog_s": args.serve_max_backlog,
+                       "threads": args.threads,
                        "cell_um": tuning.cell, "rebin_coarsen": tuning.coarsen},
             "per_rate": per_rate, "substrate_generation_s": sgen,
             "plain": {"value": plain_value, "unit": "walker-steps/s", "requests_timed": len(sample),

@@ -38,6 +38,12 @@ device memory completes at once with ``error`` set; ``cancel`` withdraws a
 waiting or resident request between rounds; a request with a deadline
 (seconds after arrival, a host-side watchdog checked every round) that is
 not done by then is cancelled with an error.  The other requests go on.
+
+Overload: with ``max_backlog_s`` set, a request is shed at submission (it
+completes at once with ``shed`` and ``error`` set) when the walker-steps
+already waiting or resident plus its own would take longer than that at the
+throughput of the recent rounds; without it every request waits its turn,
+and above the device's throughput the wait grows with the backlog.
 """
 from __future__ import annotations
 
@@ -66,11 +72,22 @@ class Ticket:
     signal: np.ndarray = None
     error: str = None
     deadline: float = None
+    shed: bool = False
     job: dict = field(default=None, repr=False)
 
     @property
     def latency(self):
         return None if self.completed is None else self.completed - self.arrival
+
+
+def would_shed(backlog_walker_steps: float, request_walker_steps: float, rate: float | None,
+               max_backlog_s: float | None) -> bool:
+    """True when the backlog plus the request would take longer than
+    max_backlog_s at `rate` walker-steps/s (never before a rate is known,
+    nor without a limit)."""
+    if max_backlog_s is None or not rate:
+        return False
+    return (float(backlog_walker_steps) + float(request_walker_steps)) / float(rate) > float(max_backlog_s)
 
 
 def footprint(spec: JobSpec, tuning: Tuning) -> int:
@@ -90,8 +107,9 @@ def footprint(spec: JobSpec, tuning: Tuning) -> int:
 class Server:
     def __init__(self, tuning: Tuning | None = None, threads: int = 128, hbm_budget: int = 40 << 30,
                  cache: SubstrateCache | None = None, round_s: float = 0.05, min_steps: int = 100,
-                 max_steps: int = 4000):
+                 max_steps: int = 4000, max_backlog_s: float | None = None):
         engine.require_cuda()
+        self.max_backlog_s = max_backlog_s
         self.tuning = tuning or Tuning()
         self.threads = threads
         if cache is None:
@@ -132,8 +150,18 @@ class Server:
         if deadline_s is not None:
             t.deadline = t.arrival + float(deadline_s)
         self.next_id += 1
+        if self.max_backlog_s is not None and would_shed(self.backlog_walker_steps(), spec.walker_steps, self.rate,
+                                                         self.max_backlog_s):
+            t.shed = True
+            self._fail(t, f"shed: the backlog exceeds {self.max_backlog_s:.3g} s at the current throughput")
+            return t
         self.waiting.append(t)
         return t
+
+    def backlog_walker_steps(self) -> int:
+        """Walker-steps of the waiting and resident requests still to run."""
+        ws = sum(t.spec.walker_steps for t in self.waiting)
+        return ws + sum(t.job["N"] * (t.job["nsteps"] - t.job["offset"]) for t in self.resident)
 
     def _fail(self, t: Ticket, why: str):
         t.error = why

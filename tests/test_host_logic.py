@@ -242,3 +242,14 @@ def test_stream_substrates_generated_in_workers_equal_in_process(tmp_path, monke
     by_key = {}
     for r in reqs:
         assert by_key.setdefault(r.spec.key, r.spec.substrate) is r.spec.substrate
+
+
+def test_shedding_rule():
+    """A request is shed when backlog plus request exceed the limit at the
+    measured rate; never without a limit or before a rate is known."""
+    from nozomi_b200.serve import would_shed
+    assert not would_shed(1e12, 1e9, None, 1.0)       # no rate yet
+    assert not would_shed(1e12, 1e9, 1e10, None)      # no limit
+    assert not would_shed(4e9, 1e9, 1e10, 1.0)        # 0.5 s of work
+    assert would_shed(1e10, 1e9, 1e10, 1.0)           # 1.1 s of work
+    assert not would_shed(9e9, 1e9, 1e10, 1.0)       # exactly 1 s: kept

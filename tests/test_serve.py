@@ -155,3 +155,23 @@ def test_cancel_deadline_oom_and_invalid_substrate_fail_alone(monkeypatch):
         assert t.error is None
         alone = BatchRun([sp], tuning=tuning, threads=64, cache=cache).step().signals()[0]
         np.testing.assert_allclose(t.signal, alone, rtol=0, atol=1e-12)
+
+
+def test_overload_sheds_new_requests_and_serves_the_rest():
+    """With max_backlog_s, requests arriving while the backlog already needs
+    longer than that are shed at once (shed and error set, no device work);
+    the others are served and equal their result alone."""
+    from nozomi_b200.batch import BatchRun, SubstrateCache
+    from nozomi_b200.serve import Server
+    from nozomi_b200.simulate import Tuning
+    tuning = Tuning(steps_per_launch=150)
+    srv = Server(tuning=tuning, threads=128, min_steps=150, max_steps=150, max_backlog_s=1e-6)
+    first = srv.submit(_spec(0, 10, 3000, 600, 6))  # no rate measured yet: admitted
+    srv.round()
+    assert srv.rate and srv.backlog_walker_steps() > 0
+    late = [srv.submit(_spec(i, 12, 4000, 600, 7)) for i in range(1, 4)]  # 1 us of backlog is exceeded
+    srv.drain()
+    assert first.error is None and not first.shed
+    assert all(t.shed and t.error.startswith("shed") and t.signal is None for t in late)
+    alone = BatchRun([first.spec], tuning=tuning, threads=64, cache=SubstrateCache()).step().signals()[0]
+    np.testing.assert_allclose(first.signal, alone, rtol=0, atol=1e-12)
