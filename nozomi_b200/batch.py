@@ -178,9 +178,11 @@ def launch_batch(table, n_jobs: int, items, lk: int, s0: int, s1: int, queue_ptr
         L.check(lib.nz_walk_batch(*args, stream), "nz_walk_batch")
 
 
-def _items(jobs, active, threads, s0, k) -> torch.Tensor:
-    """Items (job, first walker, count) of the active jobs, longest remaining
-    work first (ties in job, then walker order)."""
+def item_table(jobs, active, threads, s0, k) -> np.ndarray:
+    """[n, 3] int32 items (job, first walker, count) of the active jobs: each
+    job's walkers in runs of at most `threads`, longest remaining work
+    (walkers x steps of this chunk, [s0, s0 + k) clamped to the job) first,
+    ties in job, then walker order."""
     parts, work = [], []
     for j in active:
         N = int(jobs[j]["N"])
@@ -190,10 +192,14 @@ def _items(jobs, active, threads, s0, k) -> torch.Tensor:
         parts.append(np.stack([np.full(first.size, j), first, count], axis=1))
         work.append(steps * count)
     if not parts:
-        return torch.zeros((0, 3), dtype=torch.int32, device="cuda")
+        return np.zeros((0, 3), np.int32)
     it, w = np.concatenate(parts), np.concatenate(work)
-    it = it[np.argsort(-w, kind="stable")].astype(np.int32)
-    return torch.from_numpy(np.ascontiguousarray(it)).cuda()
+    return np.ascontiguousarray(it[np.argsort(-w, kind="stable")].astype(np.int32))
+
+
+def _items(jobs, active, threads, s0, k) -> torch.Tensor:
+    """item_table on the current GPU."""
+    return torch.from_numpy(item_table(jobs, active, threads, s0, k)).cuda()
 
 
 class BatchRun:

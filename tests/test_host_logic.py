@@ -253,3 +253,30 @@ def test_shedding_rule():
     assert not would_shed(4e9, 1e9, 1e10, 1.0)        # 0.5 s of work
     assert would_shed(1e10, 1e9, 1e10, 1.0)           # 1.1 s of work
     assert not would_shed(9e9, 1e9, 1e10, 1.0)       # exactly 1 s: kept
+
+
+def test_batch_item_table_covers_every_walker_longest_first():
+    """Each active job's walkers in runs of at most `threads`, every walker
+    once; items ordered by remaining work (walkers x this chunk's steps,
+    clamped to the job), ties in job then walker order; inactive jobs and
+    empty activity give no items."""
+    from nozomi_b200.batch import item_table
+    jobs = [{"N": 1000, "nsteps": 3000}, {"N": 300, "nsteps": 800}, {"N": 129, "nsteps": 5000},
+            {"N": 5000, "nsteps": 100}]
+    it = item_table(jobs, [0, 1, 2], 128, 500, 1000)
+    assert it.dtype == np.int32 and it.shape[1] == 3
+    for j in (0, 1, 2):
+        mine = it[it[:, 0] == j]
+        cover = np.zeros(jobs[j]["N"], int)
+        for _, first, count in mine:
+            assert 1 <= count <= 128
+            cover[first:first + count] += 1
+        assert (cover == 1).all()
+    assert not (it[:, 0] == 3).any()
+    steps = np.minimum(1000, np.array([jobs[j]["nsteps"] - 500 for j in it[:, 0]]))
+    work = steps * it[:, 2]
+    assert (np.diff(work) <= 0).all()
+    for i in range(len(it) - 1):  # ties keep job, then walker order
+        if work[i] == work[i + 1]:
+            assert (it[i, 0], it[i, 1]) < (it[i + 1, 0], it[i + 1, 1])
+    assert item_table(jobs, [], 128, 0, 100).shape == (0, 3)
