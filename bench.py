@@ -83,14 +83,14 @@ PROFILED = {
     "packed": {"kernel_sha": "f9ddf04e9e187c30", "warp_inst_per_walker_step": 56.421,
                "dram_bytes_per_walker_step": 0.9975,
                "shape": {"cell": 0.5, "near_margin": 0.5, "coarsen": 8, "threads": 128, "lists": "index",
-                         "near_shape": "round"},
+                         "near_shape": "round", "stage": 0},
                "capture": "walk_fused_kernel<PHI, idx16> launch 3 of `python bench.py --workload packed --walkers "
                           "1000000 --steps-per-launch 200 --steps 1 --warmup 1 --no-cpu-baseline --e2e-steps 0` "
                           "(200,000,000 walker-steps): 11,284,186,998 warp instructions, 199.5 MB DRAM"},
     "batched": {"kernel_sha": "f9ddf04e9e187c30", "warp_inst_per_walker_step": 41.074,
                 "dram_bytes_per_walker_step": 0.2405,
                 "shape": {"cell": 1.0, "near_margin": 0.5, "coarsen": 4, "threads": 256, "lists": "index",
-                          "near_shape": "round"},
+                          "near_shape": "round", "stage": 0},
                 "capture": "walk_fused_kernel<PHI, idx16> launch 2 of `python bench.py --walker-scale 0.1 --steps 1 "
                            "--warmup 1 --no-serving --no-plain --no-cpu-baseline --e2e-steps 0 --no-autotune --cell 1.0 "
                            "--coarsen 4 --steps-per-launch 2000 --threads 256` (64 jobs, 2,407,477,000 walker-steps): "
@@ -678,7 +678,7 @@ def run_packed(args):
         roof_issue, roof_fp32, roof_hbm = rooflines(
             "packed", kernel_ws_s, per_launch_ws, walk_launch_ms, N * 128, clk, sms, fp32_peak_tflops, F_alg, wk,
             shape={"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": 128,
-                   "lists": tuning.lists, "near_shape": tuning.near_shape})
+                   "lists": tuning.lists, "near_shape": tuning.near_shape, "stage": 0})
         line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -934,7 +934,7 @@ def run_batched(args):
     ws_launch = sum(chunk_ws) / max(len(chunk_ws), 1)
     state_bytes = 128 * sum(c["sort_walkers"] for c in run.chunks) / max(len(run.chunks), 1)
     shape = {"cell": tuning.cell, "near_margin": tuning.near_margin, "coarsen": tuning.coarsen, "threads": threads,
-             "lists": tuning.lists, "near_shape": tuning.near_shape}
+             "lists": tuning.lists, "near_shape": tuning.near_shape, "stage": tuning.stage}
     if world > 1:
         if rank == 0:
             # the issue roofline of rank 0's own batched launches (the host-core

@@ -131,3 +131,4 @@ def test_committed_counts_match_the_committed_kernel():
     for name, prof in bench.PROFILED.items():
         assert prof["kernel_sha"] == bench.kernel_sha(), name
         assert prof["shape"]["lists"] == "index" and prof["shape"]["near_shape"] == "round", name
+        assert prof["shape"]["stage"] == 0, name  # captured on the unstaged kernel
